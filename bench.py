@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Throughput of the MPDATA step on B200: Gcell-steps/s and HBM roofline.
+
+Workload (the single-grid roofline configuration): 512 x 512 x 256 FP32,
+IORD 3 with the nonoscillatory limiter, steady streamfunction flow (8 seeded
+Fourier modes + z-shear, max Courant 0.4), lognormal field smoothed by a
+5-point box filter.  Synthetic, seeded (mpdata_b200/workloads.py).  Every
+field is 268 MB, larger than the 126 MB L2, so no L2 flush is needed between
+steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0.  value: interior cell-steps per second over all
+ranks (each rank steps its own grid: replicas, weak scaling), timed with
+CUDA events on the solver's stream, max over ranks.  e2e: the same metric
+through the reference-compatible smolar() C-ABI call with pinned host
+buffers (velocity and field uploads, newest and previous field downloads
+inside the timed region).  roofline: the fused corrective-pass kernel's
+algorithmic bytes per launch over its CUDA-event launch time.  cpu_baseline:
+the reference's own smolar() (compiled from its sources with its CMake
+flags, oracle/_ref) on the host cores.
+
+--impl reference runs only that CPU reference path (rank 0) and prints its
+line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-steps/s & % HBM roofline on 1 B200, plain vs chosen at stated FP64 error"
+UNIT = "Gcell-steps/s"
+NX, NY, NS, ORDER = 512, 512, 256, 3
+CELLS = (NX - 2) * (NY - 2) * (NS - 2)
+FIELD_BYTES = NX * NY * NS * 4
+# Algorithmic bytes per interior cell (FP32, d = 3, IORD 3, limiter on):
+#   donor pass        reads c^n + 3 faces, writes c^(1)                      5
+#   corrective pass 1 reads c^(1), c^n, 3 faces; writes c^(2) + 3 faces      9
+#   corrective pass 2 reads c^(2), c^n, 3 faces; writes c^(3)                6
+B_DONOR, B_CORR_FACES, B_CORR_LAST = 5 * 4, 9 * 4, 6 * 4
+B_STEP = B_DONOR + B_CORR_FACES + B_CORR_LAST  # 80 B per cell-step
+FALLBACK_HBM_GBS = 6650.0
+CONFIG_TEXT = "roofline: 512x512x256 FP32, IORD 3 + nonoscillatory limiter, streamfunction flow"
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def traffic_from_profile():
+    """DRAM bytes per corrective-pass launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), p[5:]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = sorted(r[0] for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[2]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference path (the reference's own smolar, compiled from its sources)
+
+def cell_velocities(U, V, W):
+    """Cell velocities whose face averages follow the given faces (for the
+    cell-velocity smolar() API); ghost cells mirror to keep boundary faces."""
+    u = np.zeros_like(U); v = np.zeros_like(V); w = np.zeros_like(W)
+    u[:, :, 1:-1] = 0.5 * (U[:, :, :-2] + U[:, :, 1:-1])
+    u[:, :, 0] = U[:, :, 0]; u[:, :, -1] = U[:, :, -2]
+    v[:, 1:-1, :] = 0.5 * (V[:, :-2, :] + V[:, 1:-1, :])
+    v[:, 0, :] = V[:, 0, :]; v[:, -1, :] = V[:, -2, :]
+    w[1:-1] = 0.5 * (W[:-2] + W[1:-1])
+    w[0] = W[0]; w[-1] = W[-2]
+    return u, v, w
+
+
+def cpu_reference(steps: int, warmup: int, threads: int | None = None):
+    """Reference smolar() (FP32, -ffast-math -O3 build) on the host cores:
+    `threads` independent z-slab instances of the roofline grid, 32 interior
+    planes each (the sample), one smolar call per instance per step."""
+    import ctypes as C
+
+    import oracle
+    if not oracle.ref_available("f32_fast"):
+        return None
+    lib = oracle.ref_lib("f32_fast")
+    T = threads or min(os.cpu_count() or 1, 64)
+    planes = 32
+    wl = _workload()
+    u, v, w = cell_velocities(wl["U"], wl["V"], wl["W"])
+    insts = []
+    for t in range(T):
+        z0 = (t * planes) % (NS - planes - 2)
+        sl = slice(z0, z0 + planes + 2)
+        arrs = {k: np.ascontiguousarray(a[sl], np.float32) for k, a in
+                (("u", u), ("v", v), ("w", w), ("c0", wl["c0"]))}
+        arrs["c1"] = np.zeros_like(arrs["c0"])
+        insts.append(arrs)
+    dx = np.ones(NX, np.float32); dy = np.ones(NY, np.float32); ds = np.ones(planes + 2, np.float32)
+    P = C.POINTER(C.c_float)
+
+    def run(inst, nsteps):
+        p0 = C.cast(inst["c0"].ctypes.data, P)
+        p1 = C.cast(inst["c1"].ctypes.data, P)
+        vel = [inst[k].ctypes.data_as(P) for k in ("u", "u", "v", "v", "w", "w")]
+        for _ in range(nsteps):
+            lib.smolar(NX, NY, planes + 2, dx.ctypes.data_as(P), dy.ctypes.data_as(P),
+                       ds.ctypes.data_as(P), C.c_float(1.0), *vel, C.byref(p0), C.byref(p1), 1,
+                       ORDER)
+            p0, p1 = p1, p0
+
+    def run_all(nsteps):
+        th = [threading.Thread(target=run, args=(i, nsteps)) for i in insts]
+        t0 = time.perf_counter()
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        return time.perf_counter() - t0
+
+    if warmup:
+        run_all(warmup)
+    dt = run_all(steps)
+    cells = T * (NX - 2) * (NY - 2) * planes
+    rate = cells * steps / dt / 1e9
+    return {"value": rate, "unit": UNIT, "cores": T, "kind": "reference",
+            "sample": f"{T} thread(s) x independent {NX}x{NY}x{planes + 2} z-slab of the "
+                      f"roofline grid, IORD {ORDER}, reference smolar() built with its CMake "
+                      f"flags (-ffast-math -O3; the reference has no limiter), {steps} step(s)",
+            "seconds": dt}
+
+
+# ---------------------------------------------------------------------------
+# GPU
+
+_WL = None
+
+
+def _workload():
+    global _WL
+    if _WL is None:
+        from mpdata_b200 import workloads
+        wl = workloads.roofline(NX, NY, NS)
+        _WL = {k: (v.astype(np.float32) if isinstance(v, np.ndarray) else v)
+               for k, v in wl.items()}
+    return _WL
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_gpu(args):
+    import datetime
+
+    import torch
+    import mpdata_b200 as m
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    wl = _workload()
+    stream = torch.cuda.current_stream()
+    s = m.Solver(NX, NY, NS, order=ORDER, limiter=True)
+    s.set_stream(stream.cuda_stream)
+    s.set_faces(wl["U"], wl["V"], wl["W"])
+    s.set_field(wl["c0"])
+    s.step(args.warmup)
+    torch.cuda.synchronize()
+    s.enable_pass_timing(True)
+    s.pass_times(reset=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.step(1)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([t_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+        dist.barrier()
+    ms, n = s.pass_times()
+    s.enable_pass_timing(False)
+    mn, nneg = s.min()
+    launches = s.launches_per_step() * args.steps
+    value = world * CELLS * args.steps / (t_ms * 1e-3) / 1e9
+
+    # e2e through the reference-facing smolar() with pinned host buffers
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        e2e = run_e2e(m, args)
+    s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+
+    peak, peak_kind = hbm_peak()
+    corr_bytes = (n[1] * B_CORR_FACES + n[2] * B_CORR_LAST) * CELLS
+    corr_ms = ms[1] + ms[2]
+    achieved = corr_bytes / (corr_ms * 1e-3) / 1e9 if corr_ms > 0 else None
+    traffic = traffic_from_profile()
+    step_gbs = B_STEP * CELLS * args.steps / (t_ms * 1e-3) / 1e9 / 1  # per GPU
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": CONFIG_TEXT, "nx": NX, "ny": NY, "ns": NS, "order": ORDER,
+                   "limiter": True, "interior_cells": CELLS,
+                   "l2": "inputs larger than L2 (268 MB per field); no flush",
+                   "parallelism": f"replicas x{world} (one grid per GPU)" if world > 1 else "single GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": traffic, "peak_source": f"{peak_kind} hbm_gbs",
+                     "kernel": "k_pass_fused<float, limiter> (corrective pass)",
+                     "bytes_per_launch": {"writes_faces": B_CORR_FACES * CELLS,
+                                          "last_pass": B_CORR_LAST * CELLS},
+                     "launch_ms": {"donor": ms[0] / max(n[0], 1),
+                                   "corrective_writes_faces": ms[1] / max(n[1], 1),
+                                   "corrective_last": ms[2] / max(n[2], 1)},
+                     "step": {"bytes_per_cell_step": B_STEP, "achieved": step_gbs,
+                              "frac": step_gbs / peak}},
+        "gpu_launches": launches,
+        "positivity": {"min": mn, "negative_cells": nneg},
+    }
+    if clk:
+        line["clocks"] = clk
+    if e2e:
+        line["e2e"] = e2e
+    if world == 1 and not args.no_cpu:
+        cb = cpu_reference(steps=2, warmup=1)
+        if cb:
+            line["cpu_baseline"] = cb
+    return line
+
+
+def run_e2e(m, args):
+    """Same workload through smolar() (the drop-in entry point) with pinned
+    host arrays; per step: upload of the 3 distinct velocity arrays + field,
+    download of the newest field and the previous level."""
+    import ctypes as C
+
+    wl = _workload()
+    u, v, w = cell_velocities(wl["U"], wl["V"], wl["W"])
+
+    def pinned(a):
+        p = m.library().mpdata_host_alloc(a.nbytes)
+        if not p:
+            raise MemoryError("pinned allocation failed")
+        buf = np.ctypeslib.as_array((C.c_float * a.size).from_address(p)).reshape(a.shape)
+        buf[...] = a
+        return buf, p
+
+    bufs = [pinned(x) for x in (u, v, w, wl["c0"], np.zeros_like(wl["c0"]))]
+    hu, hv, hw, c0, c1 = (b for b, _ in bufs)
+    dx = np.ones(NX, np.float32); dy = np.ones(NY, np.float32); ds = np.ones(NS, np.float32)
+    m.set_default_options(m.SolverOptions(limiter=True))
+    steps = max(1, min(args.steps, args.e2e_steps))
+    try:
+        for it in range(2 + steps):
+            if it == 2:
+                t0 = time.perf_counter()
+            a, b = m.smolar(NX, NY, NS, dx, dy, ds, 1.0, hu, hu, hv, hv, hw, hw, c0, c1,
+                            order=ORDER)
+            c0, c1 = b, a  # driver exchange (reference tests/ring2d/test.c:104-105)
+        dt = time.perf_counter() - t0
+    finally:
+        m.set_default_options(None)
+        for _, p in bufs:
+            m.library().mpdata_host_free(C.c_void_p(p))
+    h2d = 4 * FIELD_BYTES + (NX + NY + NS) * 4
+    return {"value": CELLS * steps / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": 2 * FIELD_BYTES, "steps": steps,
+            "api": "smolar() C ABI, pinned host buffers, wall clock"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return None
+    cb = cpu_reference(steps=args.steps, warmup=args.warmup)
+    if cb is None:
+        return {"impl": "reference",
+                "unavailable": "reference build oracle/_ref/libref_f32_fast.so missing"}
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": cb["seconds"] / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": CONFIG_TEXT, "nx": NX, "ny": NY, "ns": NS, "order": ORDER,
+                       "limiter": False, "note": "the reference has no limiter"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "gpu_launches": 0}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    line = run_reference(args) if args.impl == "reference" else run_gpu(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

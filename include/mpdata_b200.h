@@ -1,0 +1,200 @@
+/* mpdata_b200 -- MPDATA transport step on NVIDIA B200 (sm_100a).
+ *
+ * C ABI.  Plain pointers and sizes only.  Two groups of entry points:
+ *
+ *  1. Drop-in replacements for the reference library's public API
+ *     (apc-llc/mpdata smolar.h).  Same names, argument meaning, host-memory
+ *     arrays and pointer-swap behaviour; `real` is float, as in the
+ *     reference's default build (CMakeLists.txt:5 adds -DSINGLE).  The
+ *     double-precision build of the reference corresponds to the *_f64
+ *     twins.  Each call stages its inputs to the GPU and the results back.
+ *
+ *  2. A device-resident handle API (mpdata_*) for stepping without host
+ *     round trips: fields stay in HBM between steps, advective faces are
+ *     computed once per velocity update, and every step is a fixed sequence
+ *     of kernel launches on the handle's stream.
+ *
+ * Memory layout of every full-grid array (both groups): nx*ny*ns elements,
+ * x fastest, a[(k*ny + j)*nx + i]; the outer one-cell shell is the fixed
+ * boundary and only cells 1..n-2 of each axis are updated
+ * (reference core/src/smolar_pass.c:30-34, core/src/smolar.c:5-31).
+ *
+ * Return values: 0 on success, a negative MPDATA_ERR_* code otherwise; the
+ * text of the last error on the calling thread is in mpdata_last_error().
+ * (The reference always returns 0, core/src/smolar.c:62.)
+ */
+#ifndef MPDATA_B200_H
+#define MPDATA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Flow-type values accepted (and, as in the reference, not used). smolar.h:3-4 */
+#define SOLENOIDAL 0
+#define DIVERGENT 1
+
+/* msmolar execution modes (accepted and ignored, as in the reference). smolar.h:53-63 */
+#define MSMOLAR_SERIAL 0
+#define MSMOLAR_PTHREADS 1
+#define MSMOLAR_OPENMP 2
+
+#define MPDATA_OK 0
+#define MPDATA_ERR_ARG (-1)      /* bad dimensions, order, pointer or option */
+#define MPDATA_ERR_CUDA (-2)     /* a CUDA runtime call failed */
+#define MPDATA_ERR_NOMEM (-3)    /* device or host allocation failed */
+#define MPDATA_ERR_COURANT (-4)  /* |face Courant number| > 1 (when checking is on) */
+#define MPDATA_ERR_STATE (-5)    /* call out of order (e.g. step before set_field) */
+
+/* ---- 1. Reference-compatible entry points --------------------------------
+ *
+ * One MPDATA step: `order` passes (1 = donor cell only, each further pass an
+ * antidiffusive correction).  On return *c1 points to the newest field and
+ * *c0 to the field before the last pass; the two pointers are exchanged iff
+ * `order` is even, and both buffers are written (reference
+ * core/src/smolar.c:44-58).  dx has nx entries (0..nx-2 used), dy ny, ds ns.
+ * u0/u1 (v, w alike) are the cell velocities at the previous and current time
+ * level; the same array may be passed twice.
+ *
+ * Replaces smolar() declared at reference smolar.h:45-48. */
+int smolar(int nx, int ny, int ns, float* dx, float* dy, float* ds, const float dt,
+           float* u0, float* u1, float* v0, float* v1, float* w0, float* w1,
+           float** c0, float** c1, int flow_type, int order);
+
+/* Double-precision twin: the reference's smolar() built with -DDOUBLE
+ * (smolar.h:10-12). */
+int smolar_f64(int nx, int ny, int ns, double* dx, double* dy, double* ds,
+               const double dt, double* u0, double* u1, double* v0, double* v1,
+               double* w0, double* w1, double** c0, double** c1, int flow_type,
+               int order);
+
+/* Decomposed step over an sx*sy*ss block grid.  *desc is created on the
+ * first call (pass a NULL-initialised void*), holds the per-block device
+ * state between calls and is released by msmolar_free().  Every step
+ * exchanges block halos deep enough for all `order` passes, so the result
+ * equals smolar() on the whole grid (the reference's intent; its own 1-cell
+ * halo does not achieve that).  The caller's *c0/*c1 pointers are exchanged
+ * the way smolar() exchanges them, and the caller's arrays are brought up to
+ * date only by msmolar_gather().  flow_type and mode are ignored.
+ *
+ * Replaces msmolar() declared at reference smolar.h:95-99. */
+int msmolar(void** desc, int nx, int ny, int ns, float* dx, float* dy, float* ds,
+            const float dt, float* u0, float* u1, float* v0, float* v1, float* w0,
+            float* w1, float** c0, float** c1, int flow_type, int order, int sx, int sy,
+            int ss, int mode);
+
+/* Copy the decomposed state's newest field into *c1 (and the field before
+ * the last pass into *c0).  Replaces msmolar_gather() declared at reference
+ * smolar.h:132-136. */
+int msmolar_gather(void** desc, int nx, int ny, int ns, float* dx, float* dy, float* ds,
+                   const float dt, float* u0, float* u1, float* v0, float* v1,
+                   float* w0, float* w1, float** c0, float** c1, int flow_type,
+                   int order, int sx, int sy, int ss, int mode);
+
+/* Release the state created by msmolar() and set *desc to NULL.  No reference
+ * counterpart (the reference never frees it, core/src/msmolar.c:25-32). */
+int msmolar_free(void** desc);
+
+/* Text of the last error raised on the calling thread ("" if none). */
+const char* mpdata_last_error(void);
+
+struct mpdata_options;
+/* Options used by smolar(), smolar_f64() and msmolar() on the calling thread
+ * (NULL restores the defaults: reference behaviour, fused kernels).  No
+ * reference counterpart: the reference has no run-time options. */
+int mpdata_set_default_options(const struct mpdata_options* opts);
+
+/* ---- 2. Device-resident handle API ---------------------------------------- */
+
+typedef struct mpdata_solver* mpdata_handle;
+
+#define MPDATA_F32 0
+#define MPDATA_F64 1
+
+/* Where a pointer argument lives. */
+#define MPDATA_HOST 0
+#define MPDATA_DEVICE 1
+
+/* Divergent-flow term of the antidiffusive velocity. */
+#define MPDATA_DIV_REFERENCE 0 /* as the reference codes it (uu.c:81-84, vv.c:85-89, ww.c:88-92) */
+#define MPDATA_DIV_OFF 1
+
+typedef struct mpdata_options {
+    int limiter;        /* 1: nonoscillatory (FCT) limiter on every corrective pass */
+    int precision_form; /* 1 (F32 only): limiter ratios in FP64 (FP32 storage form) */
+    int div_mode;       /* MPDATA_DIV_* */
+    int vv_fix;         /* 1: compute the y-face column i=1 the reference leaves
+                           unwritten (vv.c:81-82) instead of its buffer rule */
+    int strict;         /* 1: no FMA contraction; bit-identical to a strict-IEEE
+                           CPU build of the reference arithmetic */
+    int kernel;         /* 0: fused per-pass kernels (default); 1: one kernel per
+                           reference function (slower; cross-check path) */
+    int check_courant;  /* 1: reject advective faces with |Courant| > 1 */
+} mpdata_options;
+
+/* Fill *o with the defaults (all zero: reference behaviour, fused kernels). */
+void mpdata_default_options(mpdata_options* o);
+
+int mpdata_create(mpdata_handle* h, int nx, int ny, int ns, int dtype, int order,
+                  const mpdata_options* opts);
+int mpdata_destroy(mpdata_handle h);
+
+/* Use the given cudaStream_t (NULL = the legacy default stream) for all work
+ * of this handle.  The handle creates its own non-blocking stream otherwise. */
+int mpdata_set_stream(mpdata_handle h, void* stream);
+
+/* Velocities as in smolar() (six full-grid arrays of the handle's dtype plus
+ * dx, dy, ds and dt); the advective faces are computed on the GPU.
+ * `where` tells whether the pointers are host or device memory. */
+int mpdata_set_velocity(mpdata_handle h, const void* dx, const void* dy, const void* ds,
+                        double dt, const void* u0, const void* u1, const void* v0,
+                        const void* v1, const void* w0, const void* w1, int where);
+
+/* Advective face Courant numbers directly, each a full-grid array where the
+ * entry (i,j,k) is the face on the high side of cell (i,j,k) along the axis:
+ * U between cells i and i+1 (used for i 0..nx-2, j and k interior), V between
+ * j and j+1 (j 0..ny-2), W between k and k+1 (k 0..ns-2). */
+int mpdata_set_faces(mpdata_handle h, const void* U, const void* V, const void* W,
+                     int where);
+
+/* Concentration field (full grid, shell included). */
+int mpdata_set_field(mpdata_handle h, const void* c, int where);
+int mpdata_get_field(mpdata_handle h, void* c, int where);
+/* The field before the last pass of the latest step (what smolar() leaves in *c0). */
+int mpdata_get_previous(mpdata_handle h, void* c, int where);
+
+/* Advance nsteps steps on the handle's stream (asynchronous). */
+int mpdata_step(mpdata_handle h, int nsteps);
+
+/* Wait for the handle's stream. */
+int mpdata_sync(mpdata_handle h);
+
+/* Interior mass in FP64 with compensated summation (synchronous). */
+int mpdata_mass(mpdata_handle h, double* mass);
+
+/* Minimum over the interior cells and the number of negative cells (synchronous). */
+int mpdata_min(mpdata_handle h, double* minval, long long* nneg);
+
+/* Kernel launches a single mpdata_step(h, 1) issues. */
+int mpdata_launches_per_step(mpdata_handle h);
+
+/* Per-pass kernel timing with CUDA events on the handle's stream (for the
+ * roofline report).  While enabled, every mpdata_step records an event pair
+ * around the donor pass and around each corrective pass.  mpdata_pass_times
+ * synchronises and returns the accumulated milliseconds and launch counts
+ * since the last reset: [0] donor pass, [1] corrective passes that also write
+ * faces, [2] the last corrective pass. */
+int mpdata_enable_pass_timing(mpdata_handle h, int on);
+int mpdata_pass_times(mpdata_handle h, double ms[3], long long launches[3], int reset);
+
+/* Page-locked host memory for fast staging (cudaMallocHost / cudaFreeHost). */
+void* mpdata_host_alloc(size_t bytes);
+void mpdata_host_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPDATA_B200_H */

@@ -1,0 +1,65 @@
+// Kernel set of one arithmetic mode.  Included by kernels_fast.cu and
+// kernels_strict.cu with MPD_NS defined as the mode's namespace.
+#include "launch.h"
+
+namespace mpd {
+namespace MPD_NS {
+
+#include "kernels_unfused.cuh"
+#include "kernels_fused.cuh"
+
+namespace {
+constexpr int kBX = 32, kBY = 8;
+inline dim3 full_grid(const Dims& d) { return dim3((d.nx + kBX - 1) / kBX, (d.ny + kBY - 1) / kBY, d.ns); }
+}  // namespace
+
+template <typename T>
+void launch_courant(const Dims& d, const T* dx, const T* dy, const T* ds, T dt, const T* u0,
+                    const T* u1, const T* v0, const T* v1, const T* w0, const T* w1, T* U,
+                    T* V, T* W, cudaStream_t s)
+{
+    k_courant<T><<<full_grid(d), dim3(kBX, kBY), 0, s>>>(d, dx, dy, ds, dt, u0, u1, v0, v1, w0,
+                                                         w1, U, V, W);
+}
+
+template <typename T>
+void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W, T* c1,
+                  int copy_shell, cudaStream_t s)
+{
+    k_donor<T><<<full_grid(d), dim3(kBX, kBY), 0, s>>>(d, c0, U, V, W, c1, copy_shell);
+}
+
+template <typename T>
+int launch_pass_unfused(const Dims& d, const PassArgs<T>& a, T* bup, T* bdn, cudaStream_t s)
+{
+    dim3 g = full_grid(d), b(kBX, kBY);
+    k_antidiff<T><<<g, b, 0, s>>>(d, a.c, a.Uo, a.Vo, a.Wo, a.Vadv, a.Un, a.Vn, a.Wn, a.pass,
+                                  a.use_div, a.vv_fix);
+    int n = 1;
+    if (a.limiter) {
+        if (a.wide)
+            k_fct_beta<T, double><<<g, b, 0, s>>>(d, a.c, a.cn, a.Un, a.Vn, a.Wn, bup, bdn);
+        else
+            k_fct_beta<T, T><<<g, b, 0, s>>>(d, a.c, a.cn, a.Un, a.Vn, a.Wn, bup, bdn);
+        k_fct_apply<T><<<g, b, 0, s>>>(d, bup, bdn, a.Un, a.Vn, a.Wn);
+        n += 2;
+    }
+    k_donor<T><<<g, b, 0, s>>>(d, a.c, a.Un, a.Vn, a.Wn, a.c_out, 1);
+    return n + 1;
+}
+
+#define MPD_INSTANTIATE(T)                                                                  \
+    template void launch_courant<T>(const Dims&, const T*, const T*, const T*, T, const T*, \
+                                    const T*, const T*, const T*, const T*, const T*, T*,   \
+                                    T*, T*, cudaStream_t);                                  \
+    template void launch_donor<T>(const Dims&, const T*, const T*, const T*, const T*, T*,  \
+                                  int, cudaStream_t);                                       \
+    template int launch_pass_unfused<T>(const Dims&, const PassArgs<T>&, T*, T*,            \
+                                        cudaStream_t);                                      \
+    template int launch_pass_fused<T>(const Dims&, const PassArgs<T>&, cudaStream_t);
+MPD_INSTANTIATE(float)
+MPD_INSTANTIATE(double)
+#undef MPD_INSTANTIATE
+
+}  // namespace MPD_NS
+}  // namespace mpd

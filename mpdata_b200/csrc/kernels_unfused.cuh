@@ -1,0 +1,253 @@
+// One kernel per reference routine, one thread per grid point.
+//
+// This is the cross-check path (mpdata_options.kernel = 1): simple enough to
+// read against the reference line by line, it runs every formula exactly as
+// the fused kernels do but through global memory, one routine at a time.
+// Included by kernels_fast.cu / kernels_strict.cu inside namespace
+// mpd::MPD_NS.
+
+// Advective face Courant numbers (uu.c:126-138, vv.c:137-149, ww.c:143-155):
+//   U(i+1/2) = ((dt/4)/dx[i]) (((u0_i + u0_{i+1}) + u1_i) + u1_{i+1})
+// Unused face entries are written as 0.
+template <typename T>
+__global__ void k_courant(Dims d, const T* __restrict__ dx, const T* __restrict__ dy,
+                          const T* __restrict__ ds, T dt, const T* __restrict__ u0,
+                          const T* __restrict__ u1, const T* __restrict__ v0,
+                          const T* __restrict__ v1, const T* __restrict__ w0,
+                          const T* __restrict__ w1, T* __restrict__ U, T* __restrict__ V,
+                          T* __restrict__ W)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z;
+    if (i >= d.nx || j >= d.ny) return;
+    long long q = cell(d, i, j, k);
+    const T quarter_dt = T(0.25) * dt;
+    bool kin = k >= 1 && k <= d.ns - 2, jin = j >= 1 && j <= d.ny - 2, iin = i >= 1 && i <= d.nx - 2;
+    T uf = T(0), vf = T(0), wf = T(0);
+    if (kin && jin && i <= d.nx - 2)
+        uf = (quarter_dt / dx[i]) * (((u0[q] + u0[q + 1]) + u1[q]) + u1[q + 1]);
+    if (kin && iin && j <= d.ny - 2)
+        vf = (quarter_dt / dy[j]) * (((v0[q] + v0[q + d.px]) + v1[q]) + v1[q + d.px]);
+    if (jin && iin && k <= d.ns - 2)
+        wf = (quarter_dt / ds[k]) * (((w0[q] + w0[q + d.pp]) + w1[q]) + w1[q + d.pp]);
+    U[q] = uf;
+    V[q] = vf;
+    W[q] = wf;
+}
+
+// Antidiffusive faces of one corrective pass, Jacobi style (pvelocity.c:22-36):
+// every new face reads the previous pass's faces Uo/Vo/Wo and the pass input c.
+//   x faces: uu.c:34-102, y faces: vv.c:37-107, z faces: ww.c:36-113.
+// Vadv holds the advective y faces, for the column i=1 that vv_pass leaves
+// unwritten (vv.c:81-82): it reads 0 on odd passes and Vadv on even ones
+// unless vv_fix is set.
+template <typename T>
+__global__ void k_antidiff(Dims d, const T* __restrict__ c, const T* __restrict__ Uo,
+                           const T* __restrict__ Vo, const T* __restrict__ Wo,
+                           const T* __restrict__ Vadv, T* __restrict__ Un, T* __restrict__ Vn,
+                           T* __restrict__ Wn, int pass, int use_div, int vv_fix)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z;
+    if (i >= d.nx || j >= d.ny) return;
+    const long long X = 1, Y = d.px, Z = d.pp;
+    const long long q = cell(d, i, j, k);
+    const int nx = d.nx, ny = d.ny, ns = d.ns;
+    const bool kin = k >= 1 && k <= ns - 2, jin = j >= 1 && j <= ny - 2, iin = i >= 1 && i <= nx - 2;
+
+    // ---- x face between i and i+1 ----
+    if (kin && jin && i <= nx - 2) {
+        T vb, wb, neg_div = T(0);
+        if (i == 0 || i == nx - 2) {
+            long long a = (i == 0) ? q + X : q;  // adjacent interior cell
+            vb = T(0.5) * (Vo[a - Y] + Vo[a]);
+            wb = T(0.5) * (Wo[a - Z] + Wo[a]);
+        } else {
+            vb = T(0.25) * (((Vo[q + X - Y] + Vo[q + X]) + Vo[q]) + Vo[q - Y]);
+            wb = T(0.25) * (((Wo[q + X - Z] + Wo[q + X]) + Wo[q]) + Wo[q - Z]);
+            if (use_div) {
+                T s = Uo[q + X] - Uo[q - X];
+                s = s + Vo[q + X - Y];
+                s = s - Vo[q + X];
+                s = s - Vo[q];
+                s = s + Vo[q - Y];
+                s = s + Wo[q + X - Z];
+                s = s - Wo[q + X];
+                s = s - Wo[q];
+                s = s + Wo[q - Z];
+                neg_div = -((T(0.25) * Uo[q]) * s);
+            } else {
+                neg_div = -T(0);
+            }
+        }
+        T n1, d1, n2, d2;
+        grad_pair(c[q + X + Y], c[q + Y], c[q - Y], c[q + X - Y], n1, d1);
+        grad_pair(c[q + X + Z], c[q + Z], c[q - Z], c[q + X - Z], n2, d2);
+        Un[q] = face_pattern(neg_div, Uo[q], c[q], c[q + X], vb, n1, d1, wb, n2, d2);
+    }
+
+    // ---- y face between j and j+1 ----
+    if (kin && iin && j <= ny - 2) {
+        T ub, wb, neg_div = T(0);
+        bool done = false;
+        if (j == 0 || j == ny - 2) {
+            long long a = (j == 0) ? q + Y : q;
+            ub = T(0.5) * (Uo[a - X] + Uo[a]);
+            wb = T(0.5) * (Wo[a - Z] + Wo[a]);
+        } else if (i == 1 && !vv_fix) {
+            Vn[q] = (pass & 1) ? T(0) : Vadv[q];
+            done = true;
+        } else {
+            ub = T(0.25) * (((Uo[q - X + Y] + Uo[q + Y]) + Uo[q]) + Uo[q - X]);
+            wb = T(0.25) * (((Wo[q + Y - Z] + Wo[q + Y]) + Wo[q]) + Wo[q - Z]);
+            if (use_div) {
+                T ul2u = (i >= 2) ? Uo[q - 2 * X + Y] : T(0);
+                T ul2 = (i >= 2) ? Uo[q - 2 * X] : T(0);
+                T s = Vo[q + Y] - Vo[q - Y];
+                s = s + Wo[q + Y - Z];
+                s = s - Wo[q + Y];
+                s = s - Wo[q];
+                s = s + Wo[q - Z];
+                s = s + Uo[q - X + Y];
+                s = s - ul2u;
+                s = s - ul2;
+                s = s + Uo[q - X];
+                neg_div = -((T(0.25) * Vo[q]) * s);
+            } else {
+                neg_div = -T(0);
+            }
+        }
+        if (!done) {
+            T n1, d1, n2, d2;
+            grad_pair(c[q + X + Y], c[q + X], c[q - X], c[q - X + Y], n1, d1);
+            grad_pair(c[q + Y + Z], c[q + Z], c[q - Z], c[q + Y - Z], n2, d2);
+            Vn[q] = face_pattern(neg_div, Vo[q], c[q], c[q + Y], ub, n1, d1, wb, n2, d2);
+        }
+    }
+
+    // ---- z face between k and k+1 ----
+    if (jin && iin && k <= ns - 2) {
+        T ub, vb, neg_div = T(0);
+        if (k == 0 || k == ns - 2) {
+            long long a = (k == 0) ? q + Z : q;
+            ub = T(0.5) * (Uo[a - X] + Uo[a]);
+            vb = T(0.5) * (Vo[a - Y] + Vo[a]);
+        } else {
+            ub = T(0.25) * (((Uo[q] + Uo[q + Z]) + Uo[q - X + Z]) + Uo[q - X]);
+            vb = T(0.25) * (((Vo[q - Y + Z] + Vo[q + Z]) + Vo[q]) + Vo[q - Y]);
+            if (use_div) {
+                T s = Wo[q + Z] - Wo[q - Z];
+                s = s + Uo[q - X + Z];
+                s = s - Uo[q + Z];
+                s = s - Uo[q];
+                s = s + Uo[q - X];
+                s = s + Vo[q - Y + Z];
+                s = s - Vo[q + Z];
+                s = s - Vo[q];
+                s = s + Vo[q - Y];
+                neg_div = -((T(0.25) * Wo[q]) * s);
+            } else {
+                neg_div = -T(0);
+            }
+        }
+        T n1, d1, n2, d2;
+        grad_pair(c[q + X + Z], c[q + X], c[q - X], c[q - X + Z], n1, d1);
+        grad_pair(c[q + Y + Z], c[q + Y], c[q - Y], c[q - Y + Z], n2, d2);
+        Wn[q] = face_pattern(neg_div, Wo[q], c[q], c[q + Z], ub, n1, d1, vb, n2, d2);
+    }
+}
+
+// Limiter ratios of every interior cell (no reference counterpart;
+// Smolarkiewicz & Grabowski 1990): bounds from c (this pass's input) and
+// cn (the step's input) over the cell and its face neighbours (z neighbours
+// only when ns > 3), in/out sums of the donor fluxes through the six faces.
+// A = accumulation type (double for the FP32-storage form).
+template <typename T, typename A>
+__global__ void k_fct_beta(Dims d, const T* __restrict__ c, const T* __restrict__ cn,
+                           const T* __restrict__ U, const T* __restrict__ V,
+                           const T* __restrict__ W, T* __restrict__ bup, T* __restrict__ bdn)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z;
+    if (i < 1 || j < 1 || k < 1 || i > d.nx - 2 || j > d.ny - 2 || k > d.ns - 2) return;
+    const long long X = 1, Y = d.px, Z = d.pp;
+    const long long q = cell(d, i, j, k);
+    T psi = c[q];
+    T mx = psi, mn = psi, t;
+#define MPD_BOUND(v) do { t = (v); mx = t > mx ? t : mx; mn = t < mn ? t : mn; } while (0)
+    MPD_BOUND(cn[q]);
+    MPD_BOUND(c[q - X]); MPD_BOUND(cn[q - X]);
+    MPD_BOUND(c[q + X]); MPD_BOUND(cn[q + X]);
+    MPD_BOUND(c[q - Y]); MPD_BOUND(cn[q - Y]);
+    MPD_BOUND(c[q + Y]); MPD_BOUND(cn[q + Y]);
+    if (d.ns > 3) {
+        MPD_BOUND(c[q - Z]); MPD_BOUND(cn[q - Z]);
+        MPD_BOUND(c[q + Z]); MPD_BOUND(cn[q + Z]);
+    }
+#undef MPD_BOUND
+    A fin = A(0), fout = A(0);
+    lim_acc(lim_flux<T, A>(U[q - X], c[q - X], psi), false, fin, fout);
+    lim_acc(lim_flux<T, A>(U[q], psi, c[q + X]), true, fin, fout);
+    lim_acc(lim_flux<T, A>(V[q - Y], c[q - Y], psi), false, fin, fout);
+    lim_acc(lim_flux<T, A>(V[q], psi, c[q + Y]), true, fin, fout);
+    lim_acc(lim_flux<T, A>(W[q - Z], c[q - Z], psi), false, fin, fout);
+    lim_acc(lim_flux<T, A>(W[q], psi, c[q + Z]), true, fin, fout);
+    bup[q] = T((A(mx) - A(psi)) / (fin + lim_tiny<A>()));
+    bdn[q] = T((A(psi) - A(mn)) / (fout + lim_tiny<A>()));
+}
+
+// Apply the limiter to every used face; shell cells count as beta = 1.
+template <typename T>
+__global__ void k_fct_apply(Dims d, const T* __restrict__ bup, const T* __restrict__ bdn,
+                            T* __restrict__ U, T* __restrict__ V, T* __restrict__ W)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z;
+    if (i >= d.nx || j >= d.ny) return;
+    const long long X = 1, Y = d.px, Z = d.pp;
+    const long long q = cell(d, i, j, k);
+    const int nx = d.nx, ny = d.ny, ns = d.ns;
+    auto in = [&](int a, int b, int c_) {
+        return a >= 1 && a <= nx - 2 && b >= 1 && b <= ny - 2 && c_ >= 1 && c_ <= ns - 2;
+    };
+    auto up = [&](long long p, bool interior) { return interior ? bup[p] : T(1); };
+    auto dn = [&](long long p, bool interior) { return interior ? bdn[p] : T(1); };
+    const bool kin = k >= 1 && k <= ns - 2, jin = j >= 1 && j <= ny - 2, iin = i >= 1 && i <= nx - 2;
+    if (kin && jin && i <= nx - 2) {
+        bool lo = in(i, j, k), hi = in(i + 1, j, k);
+        U[q] = limit_face(U[q], up(q, lo), dn(q, lo), up(q + X, hi), dn(q + X, hi));
+    }
+    if (kin && iin && j <= ny - 2) {
+        bool lo = in(i, j, k), hi = in(i, j + 1, k);
+        V[q] = limit_face(V[q], up(q, lo), dn(q, lo), up(q + Y, hi), dn(q + Y, hi));
+    }
+    if (jin && iin && k <= ns - 2) {
+        bool lo = in(i, j, k), hi = in(i, j, k + 1);
+        W[q] = limit_face(W[q], up(q, lo), dn(q, lo), up(q + Z, hi), dn(q + Z, hi));
+    }
+}
+
+// Donor-cell pass (smolar_pass.c:30-57) over the interior; with copy_shell
+// the fixed boundary shell is copied from c0 as bndcpy does (smolar.c:5-31).
+template <typename T>
+__global__ void k_donor(Dims d, const T* __restrict__ c0, const T* __restrict__ U,
+                        const T* __restrict__ V, const T* __restrict__ W, T* __restrict__ c1,
+                        int copy_shell)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y * blockDim.y + threadIdx.y;
+    int k = blockIdx.z;
+    if (i >= d.nx || j >= d.ny) return;
+    const long long X = 1, Y = d.px, Z = d.pp;
+    const long long q = cell(d, i, j, k);
+    if (i >= 1 && j >= 1 && k >= 1 && i <= d.nx - 2 && j <= d.ny - 2 && k <= d.ns - 2) {
+        c1[q] = donor_update(c0[q], c0[q - X], c0[q + X], c0[q - Y], c0[q + Y], c0[q - Z],
+                             c0[q + Z], U[q], U[q - X], V[q], V[q - Y], W[q], W[q - Z]);
+    } else if (copy_shell) {
+        c1[q] = c0[q];
+    }
+}

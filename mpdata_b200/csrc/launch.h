@@ -1,0 +1,56 @@
+// Host-side launchers of the MPDATA kernels.  kernels_all.cuh is compiled
+// twice: namespace mpd::fast (nvcc's default FMA contraction) and
+// mpd::strict (-fmad=false: bit-identical to a strict-IEEE CPU build of the
+// reference arithmetic).  Both expose the same launcher set.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace mpd {
+
+// Per-pass description for the corrective-pass launchers.
+template <typename T> struct PassArgs {
+    const T* c;        // this pass's input field (level o)
+    const T* cn;       // the step's input field (limiter bounds); may be null without limiter
+    const T* Uo;       // previous pass's faces (advective on pass 1)
+    const T* Vo;
+    const T* Wo;
+    const T* Vadv;     // advective y faces (column rule of vv.c:81-82)
+    T* Un;             // this pass's (limited) faces
+    T* Vn;
+    T* Wn;
+    T* c_out;          // level o+1
+    int pass;          // o >= 1
+    int use_div;       // divergent-flow term on
+    int vv_fix;        // compute the y-face column i=1
+    int limiter;       // FCT on
+    int wide;          // FP64 limiter ratios (float storage only)
+    int write_faces;   // the next pass reads Un/Vn/Wn
+};
+
+#define MPD_DECLARE_LAUNCHERS                                                              \
+    template <typename T>                                                                  \
+    void launch_courant(const Dims& d, const T* dx, const T* dy, const T* ds, T dt,        \
+                        const T* u0, const T* u1, const T* v0, const T* v1, const T* w0,   \
+                        const T* w1, T* U, T* V, T* W, cudaStream_t s);                    \
+    template <typename T>                                                                  \
+    void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W,      \
+                      T* c1, int copy_shell, cudaStream_t s);                              \
+    /* Corrective pass, one kernel per reference routine; bup/bdn scratch (limiter). */    \
+    template <typename T>                                                                  \
+    int launch_pass_unfused(const Dims& d, const PassArgs<T>& a, T* bup, T* bdn,           \
+                            cudaStream_t s);                                               \
+    /* Corrective pass as one fused kernel; returns launches issued. */                    \
+    template <typename T>                                                                  \
+    int launch_pass_fused(const Dims& d, const PassArgs<T>& a, cudaStream_t s);
+
+namespace fast { MPD_DECLARE_LAUNCHERS }
+namespace strict { MPD_DECLARE_LAUNCHERS }
+
+// Mode-independent utility kernels (reductions, fills), in solver.cu.
+template <typename T> void launch_mass(const Dims& d, const T* c, double* partial, int nblk,
+                                       double* out, cudaStream_t s);
+
+}  // namespace mpd

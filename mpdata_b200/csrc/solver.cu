@@ -1,0 +1,682 @@
+// Host side of the C ABI: the device-resident solver handle and the
+// reference-compatible smolar()/smolar_f64() entry points built on it.
+//
+// Step driver (reference core/src/smolar.c:33-63, re-designed for the GPU):
+//   * three field buffers rotate so the step's input c^n stays intact for the
+//     limiter bounds while passes ping-pong between the other two;
+//   * the advective faces are computed once per velocity update (the
+//     reference recomputes them on every call, smolar.c:40-42);
+//   * pseudo-velocities are Jacobi-updated between two face sets
+//     (pvelocity.c:22-36), the advective set staying untouched;
+//   * the fixed boundary shell is written into all three buffers once, when
+//     the field is set, and never changes afterwards (bndcpy, smolar.c:5-31,
+//     only ever copies it forward).
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "launch.h"
+#include "mpdata_b200.h"
+#include "solver.h"
+
+using mpd::Dims;
+
+// ---------------------------------------------------------------------------
+// errors
+namespace {
+thread_local std::string g_last_error;
+}  // namespace
+
+int mpd::fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+extern "C" const char* mpdata_last_error(void) { return g_last_error.c_str(); }
+
+#define CUDA_TRY(expr)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (expr);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return mpd::fail(MPDATA_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// reductions (mode independent)
+namespace mpd {
+namespace {
+
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs
+
+// Neumaier two-sum accumulate.
+__device__ __forceinline__ void neu_add(double& s, double& comp, double x)
+{
+    double t = s + x;
+    comp += (fabs(s) >= fabs(x)) ? (s - t) + x : (x - t) + s;
+    s = t;
+}
+
+// Per-block partials over the interior cells: compensated sum, min, count < 0.
+template <typename T>
+__global__ void k_stats(Dims d, const T* __restrict__ c, double* __restrict__ part)
+{
+    const long long nint = (long long)(d.nx - 2) * (d.ny - 2) * (d.ns - 2);
+    double s = 0, comp = 0, mn = 1e308, neg = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint;
+         t += (long long)gridDim.x * blockDim.x) {
+        int i = 1 + (int)(t % (d.nx - 2));
+        long long r = t / (d.nx - 2);
+        int j = 1 + (int)(r % (d.ny - 2));
+        int k = 1 + (int)(r / (d.ny - 2));
+        double x = (double)c[cell(d, i, j, k)];
+        neu_add(s, comp, x);
+        mn = x < mn ? x : mn;
+        neg += x < 0 ? 1.0 : 0.0;
+    }
+    __shared__ double sh[4][kRedThreads];
+    sh[0][threadIdx.x] = s;
+    sh[1][threadIdx.x] = comp;
+    sh[2][threadIdx.x] = mn;
+    sh[3][threadIdx.x] = neg;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double S = 0, Cp = 0, M = 1e308, N = 0;
+        for (int q = 0; q < kRedThreads; q++) {  // fixed order: deterministic
+            neu_add(S, Cp, sh[0][q]);
+            Cp += sh[1][q];
+            M = sh[2][q] < M ? sh[2][q] : M;
+            N += sh[3][q];
+        }
+        part[4 * blockIdx.x + 0] = S;
+        part[4 * blockIdx.x + 1] = Cp;
+        part[4 * blockIdx.x + 2] = M;
+        part[4 * blockIdx.x + 3] = N;
+    }
+}
+
+__global__ void k_stats_final(const double* __restrict__ part, int nblk, double* __restrict__ out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double S = 0, Cp = 0, M = 1e308, N = 0;
+    for (int b = 0; b < nblk; b++) {
+        neu_add(S, Cp, part[4 * b + 0]);
+        Cp += part[4 * b + 1];
+        M = part[4 * b + 2] < M ? part[4 * b + 2] : M;
+        N += part[4 * b + 3];
+    }
+    out[0] = S + Cp;
+    out[1] = M;
+    out[2] = N;
+}
+
+// max |face| over the used entries of the three face arrays.
+template <typename T>
+__global__ void k_facemax(Dims d, const T* __restrict__ U, const T* __restrict__ V,
+                          const T* __restrict__ W, double* __restrict__ part)
+{
+    const long long n = (long long)d.pp * d.ns;
+    double m = 0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        double a = fabs((double)U[t]), b = fabs((double)V[t]), c = fabs((double)W[t]);
+        m = fmax(m, fmax(a, fmax(b, c)));
+    }
+    __shared__ double sh[kRedThreads];
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_max_final(const double* __restrict__ part, int nblk, double* __restrict__ out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double m = 0;
+    for (int b = 0; b < nblk; b++) m = fmax(m, part[b]);
+    out[0] = m;
+}
+
+}  // namespace
+}  // namespace mpd
+
+// ---------------------------------------------------------------------------
+// solver
+using mpd::Solver;
+
+namespace {
+
+int check_dims(int nx, int ny, int ns)
+{
+    if (nx < 3 || ny < 3 || ns < 3)
+        return mpd::fail(MPDATA_ERR_ARG, "grid %dx%dx%d: every dimension must be >= 3", nx, ny, ns);
+    if ((long long)nx * ny * ns > (1LL << 40))
+        return mpd::fail(MPDATA_ERR_ARG, "grid %dx%dx%d too large", nx, ny, ns);
+    return 0;
+}
+
+size_t field_bytes(const Solver* h) { return (size_t)h->d.pp * h->d.ns * h->esz; }
+
+template <typename T> T* F(Solver* h, int set, int axis) { return (T*)h->faces[set][axis]; }
+template <typename T> T* Cb(Solver* h, int b) { return (T*)h->c[b]; }
+
+int ensure_device(const Solver* h)
+{
+    int cur = -1;
+    CUDA_TRY(cudaGetDevice(&cur));
+    if (cur != h->device) CUDA_TRY(cudaSetDevice(h->device));
+    return 0;
+}
+
+// Copy a dense host/device full grid (row pitch nx) into a pitched device array.
+int put_grid(Solver* h, void* dst, const void* src, int where)
+{
+    size_t w = (size_t)h->d.nx * h->esz;
+    CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)h->d.px * h->esz, src, w, w,
+                               (size_t)h->d.ny * h->d.ns,
+                               where == MPDATA_HOST ? cudaMemcpyHostToDevice
+                                                    : cudaMemcpyDeviceToDevice,
+                               h->stream));
+    return 0;
+}
+
+int get_grid(Solver* h, void* dst, const void* src, int where)
+{
+    size_t w = (size_t)h->d.nx * h->esz;
+    CUDA_TRY(cudaMemcpy2DAsync(dst, w, src, (size_t)h->d.px * h->esz, w,
+                               (size_t)h->d.ny * h->d.ns,
+                               where == MPDATA_HOST ? cudaMemcpyDeviceToHost
+                                                    : cudaMemcpyDeviceToDevice,
+                               h->stream));
+    return 0;
+}
+
+template <typename T> struct ModeOps {
+    decltype(&mpd::fast::launch_courant<T>) courant;
+    decltype(&mpd::fast::launch_donor<T>) donor;
+    decltype(&mpd::fast::launch_pass_unfused<T>) pass_unfused;
+    decltype(&mpd::fast::launch_pass_fused<T>) pass_fused;
+};
+
+template <typename T> ModeOps<T> ops(const Solver* h)
+{
+    if (h->opts.strict)
+        return {mpd::strict::launch_courant<T>, mpd::strict::launch_donor<T>,
+                mpd::strict::launch_pass_unfused<T>, mpd::strict::launch_pass_fused<T>};
+    return {mpd::fast::launch_courant<T>, mpd::fast::launch_donor<T>,
+            mpd::fast::launch_pass_unfused<T>, mpd::fast::launch_pass_fused<T>};
+}
+
+template <typename T> int check_courant(Solver* h)
+{
+    mpd::k_facemax<T><<<mpd::kRedBlocks, mpd::kRedThreads, 0, h->stream>>>(
+        h->d, F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), h->red);
+    mpd::k_max_final<<<1, 1, 0, h->stream>>>(h->red, mpd::kRedBlocks, h->red + 4 * mpd::kRedBlocks);
+    double m = 0;
+    CUDA_TRY(cudaMemcpyAsync(&m, h->red + 4 * mpd::kRedBlocks, sizeof m, cudaMemcpyDeviceToHost,
+                             h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (!(m <= 1.0))
+        return mpd::fail(MPDATA_ERR_COURANT, "max |face Courant number| = %g exceeds 1", m);
+    return 0;
+}
+
+// Event pair around one pass launch when per-pass timing is on.
+struct PassTimer {
+    Solver* h;
+    int cls;
+    cudaEvent_t a = nullptr, b = nullptr;
+    PassTimer(Solver* h_, int cls_) : h(h_), cls(cls_)
+    {
+        if (!h->timing) return;
+        a = take();
+        b = take();
+        cudaEventRecord(a, h->stream);
+    }
+    ~PassTimer()
+    {
+        if (!h->timing) return;
+        cudaEventRecord(b, h->stream);
+        h->pending[cls].push_back({a, b});
+    }
+    cudaEvent_t take()
+    {
+        cudaEvent_t e = nullptr;
+        if (!h->event_pool.empty()) {
+            e = h->event_pool.back();
+            h->event_pool.pop_back();
+        } else {
+            cudaEventCreate(&e);
+        }
+        return e;
+    }
+};
+
+template <typename T> int step_impl(Solver* h, int nsteps)
+{
+    ModeOps<T> op = ops<T>(h);
+    const Dims& d = h->d;
+    const int P = h->order;
+    const bool fused = h->opts.kernel == 0;
+    for (int s = 0; s < nsteps; s++) {
+        const int b0 = h->cur, b1 = (b0 + 1) % 3, b2 = (b0 + 2) % 3;
+        // pass 0: donor cell with the advective faces
+        {
+            PassTimer t(h, 0);
+            op.donor(d, Cb<T>(h, b0), F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), Cb<T>(h, b1), 0,
+                     h->stream);
+        }
+        int in = b1, out = b2;
+        for (int o = 1; o < P; o++) {
+            const int rs = (o == 1) ? 0 : 1 + ((o - 2) & 1);
+            const int ws = 1 + ((o - 1) & 1);
+            mpd::PassArgs<T> a;
+            a.c = Cb<T>(h, in);
+            a.cn = Cb<T>(h, b0);
+            a.Uo = F<T>(h, rs, 0);
+            a.Vo = F<T>(h, rs, 1);
+            a.Wo = F<T>(h, rs, 2);
+            a.Vadv = F<T>(h, 0, 1);
+            a.Un = F<T>(h, ws, 0);
+            a.Vn = F<T>(h, ws, 1);
+            a.Wn = F<T>(h, ws, 2);
+            a.c_out = Cb<T>(h, out);
+            a.pass = o;
+            a.use_div = h->opts.div_mode != MPDATA_DIV_OFF;
+            a.vv_fix = h->opts.vv_fix;
+            a.limiter = h->opts.limiter;
+            a.wide = h->opts.precision_form;
+            a.write_faces = o < P - 1;
+            {
+                PassTimer timer(h, a.write_faces ? 1 : 2);
+                if (fused) op.pass_fused(d, a, h->stream);
+                else op.pass_unfused(d, a, (T*)h->bup, (T*)h->bdn, h->stream);
+            }
+            int t = in; in = out; out = t;
+        }
+        if (P == 1) { h->cur = b1; h->prev = b0; }
+        else { h->cur = in; h->prev = out; }
+    }
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+template <typename T> int launches_per_step(const Solver* h)
+{
+    int n = 1;  // donor pass
+    for (int o = 1; o < h->order; o++) {
+        if (h->opts.kernel == 0) n += 1;
+        else n += h->opts.limiter ? 4 : 2;
+    }
+    return n;
+}
+
+int alloc_solver(Solver* h)
+{
+    size_t fb = field_bytes(h);
+    for (int b = 0; b < 3; b++) CUDA_TRY(cudaMalloc(&h->c[b], fb));
+    for (int s = 0; s < 3; s++)
+        for (int a = 0; a < 3; a++) CUDA_TRY(cudaMalloc(&h->faces[s][a], fb));
+    if (h->opts.kernel != 0 && h->opts.limiter) {
+        CUDA_TRY(cudaMalloc(&h->bup, fb));
+        CUDA_TRY(cudaMalloc(&h->bdn, fb));
+    }
+    CUDA_TRY(cudaMalloc(&h->red, sizeof(double) * (4 * mpd::kRedBlocks + 8)));
+    size_t nmet = (size_t)h->d.nx + h->d.ny + h->d.ns;
+    CUDA_TRY(cudaMalloc(&h->metric, nmet * h->esz));
+    for (int b = 0; b < 3; b++) CUDA_TRY(cudaMemsetAsync(h->c[b], 0, fb, h->stream));
+    for (int s = 0; s < 3; s++)
+        for (int a = 0; a < 3; a++) CUDA_TRY(cudaMemsetAsync(h->faces[s][a], 0, fb, h->stream));
+    return 0;
+}
+
+void free_solver(Solver* h)
+{
+    for (auto& v : h->pending)
+        for (auto& p : v) {
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
+    for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
+    for (int b = 0; b < 3; b++) cudaFree(h->c[b]);
+    for (int s = 0; s < 3; s++)
+        for (int a = 0; a < 3; a++) cudaFree(h->faces[s][a]);
+    for (int v = 0; v < 6; v++) cudaFree(h->vel[v]);
+    cudaFree(h->bup);
+    cudaFree(h->bdn);
+    cudaFree(h->red);
+    cudaFree(h->metric);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+}  // namespace
+
+int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int order,
+                       const mpdata_options* opts)
+{
+    if (!out) return fail(MPDATA_ERR_ARG, "null handle pointer");
+    *out = nullptr;
+    if (int rc = check_dims(nx, ny, ns)) return rc;
+    if (dtype != MPDATA_F32 && dtype != MPDATA_F64) return fail(MPDATA_ERR_ARG, "bad dtype %d", dtype);
+    if (order < 1 || order > 64) return fail(MPDATA_ERR_ARG, "order %d outside 1..64", order);
+    mpdata_options o;
+    mpdata_default_options(&o);
+    if (opts) o = *opts;
+    if (o.precision_form && dtype != MPDATA_F32)
+        return fail(MPDATA_ERR_ARG, "precision_form applies to float storage only");
+    if (o.kernel < 0 || o.kernel > 1) return fail(MPDATA_ERR_ARG, "bad kernel option %d", o.kernel);
+    std::unique_ptr<Solver> h(new Solver());
+    h->dtype = dtype;
+    h->esz = dtype == MPDATA_F32 ? 4 : 8;
+    h->order = order;
+    h->opts = o;
+    h->d.nx = nx;
+    h->d.ny = ny;
+    h->d.ns = ns;
+    h->d.px = ((long long)nx + 31) / 32 * 32;
+    h->d.pp = h->d.px * ny;
+    CUDA_TRY(cudaGetDevice(&h->device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+    if (int rc = alloc_solver(h.get())) {
+        free_solver(h.get());
+        return rc == MPDATA_ERR_CUDA ? fail(MPDATA_ERR_NOMEM, "device allocation failed: %s",
+                                            mpdata_last_error())
+                                     : rc;
+    }
+    *out = h.release();
+    return 0;
+}
+
+void mpd::destroy_solver(Solver* h)
+{
+    if (!h) return;
+    ensure_device(h);
+    cudaStreamSynchronize(h->stream);
+    free_solver(h);
+    delete h;
+}
+
+int mpd::set_velocity(Solver* h, const void* dx, const void* dy, const void* ds, double dt,
+                      const void* const vel[6], int where)
+{
+    if (!h || !dx || !dy || !ds) return fail(MPDATA_ERR_ARG, "null argument");
+    for (int v = 0; v < 6; v++)
+        if (!vel[v]) return fail(MPDATA_ERR_ARG, "null velocity array");
+    if (int rc = ensure_device(h)) return rc;
+    const size_t fb = field_bytes(h);
+    // Stage the distinct velocity arrays (drivers pass the same array for both
+    // time levels, reference tests/ring2d/test.c:89-91).
+    const void* dev[6];
+    for (int v = 0; v < 6; v++) {
+        int same = -1;
+        for (int w = 0; w < v; w++)
+            if (vel[w] == vel[v]) same = w;
+        if (same >= 0) { dev[v] = dev[same]; continue; }
+        if (!h->vel[v]) CUDA_TRY(cudaMalloc(&h->vel[v], fb));
+        if (int rc = put_grid(h, h->vel[v], vel[v], where)) return rc;
+        dev[v] = h->vel[v];
+    }
+    const cudaMemcpyKind kind = where == MPDATA_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    char* met = (char*)h->metric;
+    CUDA_TRY(cudaMemcpyAsync(met, dx, h->d.nx * h->esz, kind, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(met + h->d.nx * h->esz, dy, h->d.ny * h->esz, kind, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(met + (h->d.nx + h->d.ny) * h->esz, ds, h->d.ns * h->esz, kind, h->stream));
+    if (h->dtype == MPDATA_F32) {
+        const float* m = (const float*)h->metric;
+        ops<float>(h).courant(h->d, m, m + h->d.nx, m + h->d.nx + h->d.ny, (float)dt,
+                              (const float*)dev[0], (const float*)dev[1], (const float*)dev[2],
+                              (const float*)dev[3], (const float*)dev[4], (const float*)dev[5],
+                              F<float>(h, 0, 0), F<float>(h, 0, 1), F<float>(h, 0, 2), h->stream);
+    } else {
+        const double* m = (const double*)h->metric;
+        ops<double>(h).courant(h->d, m, m + h->d.nx, m + h->d.nx + h->d.ny, dt,
+                               (const double*)dev[0], (const double*)dev[1], (const double*)dev[2],
+                               (const double*)dev[3], (const double*)dev[4], (const double*)dev[5],
+                               F<double>(h, 0, 0), F<double>(h, 0, 1), F<double>(h, 0, 2), h->stream);
+    }
+    CUDA_TRY(cudaGetLastError());
+    h->have_faces = true;
+    if (h->opts.check_courant)
+        return h->dtype == MPDATA_F32 ? check_courant<float>(h) : check_courant<double>(h);
+    return 0;
+}
+
+int mpd::set_faces(Solver* h, const void* U, const void* V, const void* W, int where)
+{
+    if (!h || !U || !V || !W) return fail(MPDATA_ERR_ARG, "null argument");
+    if (int rc = ensure_device(h)) return rc;
+    const void* src[3] = {U, V, W};
+    for (int a = 0; a < 3; a++)
+        if (int rc = put_grid(h, h->faces[0][a], src[a], where)) return rc;
+    h->have_faces = true;
+    if (h->opts.check_courant)
+        return h->dtype == MPDATA_F32 ? check_courant<float>(h) : check_courant<double>(h);
+    return 0;
+}
+
+int mpd::set_field(Solver* h, const void* c, int where)
+{
+    if (!h || !c) return fail(MPDATA_ERR_ARG, "null argument");
+    if (int rc = ensure_device(h)) return rc;
+    h->cur = 0;
+    h->prev = 0;
+    if (int rc = put_grid(h, h->c[0], c, where)) return rc;
+    // The shell is constant from here on: give every buffer the same one.
+    const size_t fb = field_bytes(h);
+    CUDA_TRY(cudaMemcpyAsync(h->c[1], h->c[0], fb, cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->c[2], h->c[0], fb, cudaMemcpyDeviceToDevice, h->stream));
+    h->have_field = true;
+    return 0;
+}
+
+int mpd::get_field(Solver* h, void* c, int where, bool previous)
+{
+    if (!h || !c) return fail(MPDATA_ERR_ARG, "null argument");
+    if (!h->have_field) return fail(MPDATA_ERR_STATE, "no field set");
+    if (int rc = ensure_device(h)) return rc;
+    return get_grid(h, c, h->c[previous ? h->prev : h->cur], where);
+}
+
+int mpd::step(Solver* h, int nsteps)
+{
+    if (!h) return fail(MPDATA_ERR_ARG, "null handle");
+    if (nsteps < 0) return fail(MPDATA_ERR_ARG, "negative step count");
+    if (!h->have_field || !h->have_faces)
+        return fail(MPDATA_ERR_STATE, "field and velocity/faces must be set before stepping");
+    if (int rc = ensure_device(h)) return rc;
+    return h->dtype == MPDATA_F32 ? step_impl<float>(h, nsteps) : step_impl<double>(h, nsteps);
+}
+
+int mpd::stats(Solver* h, double out[3])
+{
+    if (!h) return fail(MPDATA_ERR_ARG, "null handle");
+    if (!h->have_field) return fail(MPDATA_ERR_STATE, "no field set");
+    if (int rc = ensure_device(h)) return rc;
+    if (h->d.nx < 3 || h->d.ny < 3 || h->d.ns < 3) return fail(MPDATA_ERR_ARG, "no interior");
+    if (h->dtype == MPDATA_F32)
+        mpd::k_stats<float><<<mpd::kRedBlocks, mpd::kRedThreads, 0, h->stream>>>(
+            h->d, (const float*)h->c[h->cur], h->red);
+    else
+        mpd::k_stats<double><<<mpd::kRedBlocks, mpd::kRedThreads, 0, h->stream>>>(
+            h->d, (const double*)h->c[h->cur], h->red);
+    mpd::k_stats_final<<<1, 1, 0, h->stream>>>(h->red, mpd::kRedBlocks, h->red + 4 * mpd::kRedBlocks);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, h->red + 4 * mpd::kRedBlocks, 3 * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mpd::launches(const Solver* h)
+{
+    return h->dtype == MPDATA_F32 ? launches_per_step<float>(h) : launches_per_step<double>(h);
+}
+
+// ---------------------------------------------------------------------------
+// C ABI: handle API
+
+extern "C" {
+
+void mpdata_default_options(mpdata_options* o)
+{
+    if (o) memset(o, 0, sizeof *o);
+}
+
+int mpdata_create(mpdata_handle* h, int nx, int ny, int ns, int dtype, int order,
+                  const mpdata_options* opts)
+{
+    return mpd::create_solver(reinterpret_cast<Solver**>(h), nx, ny, ns, dtype, order, opts);
+}
+
+int mpdata_destroy(mpdata_handle h)
+{
+    mpd::destroy_solver(reinterpret_cast<Solver*>(h));
+    return 0;
+}
+
+int mpdata_set_stream(mpdata_handle hh, void* stream)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h) return mpd::fail(MPDATA_ERR_ARG, "null handle");
+    if (int rc = ensure_device(h)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)stream;
+    h->own_stream = false;
+    return 0;
+}
+
+int mpdata_set_velocity(mpdata_handle h, const void* dx, const void* dy, const void* ds,
+                        double dt, const void* u0, const void* u1, const void* v0,
+                        const void* v1, const void* w0, const void* w1, int where)
+{
+    const void* vel[6] = {u0, u1, v0, v1, w0, w1};
+    return mpd::set_velocity(reinterpret_cast<Solver*>(h), dx, dy, ds, dt, vel, where);
+}
+
+int mpdata_set_faces(mpdata_handle h, const void* U, const void* V, const void* W, int where)
+{
+    return mpd::set_faces(reinterpret_cast<Solver*>(h), U, V, W, where);
+}
+
+int mpdata_set_field(mpdata_handle h, const void* c, int where)
+{
+    return mpd::set_field(reinterpret_cast<Solver*>(h), c, where);
+}
+
+int mpdata_get_field(mpdata_handle h, void* c, int where)
+{
+    int rc = mpd::get_field(reinterpret_cast<Solver*>(h), c, where, false);
+    if (rc) return rc;
+    return mpdata_sync(h);
+}
+
+int mpdata_get_previous(mpdata_handle h, void* c, int where)
+{
+    int rc = mpd::get_field(reinterpret_cast<Solver*>(h), c, where, true);
+    if (rc) return rc;
+    return mpdata_sync(h);
+}
+
+int mpdata_step(mpdata_handle h, int nsteps)
+{
+    return mpd::step(reinterpret_cast<Solver*>(h), nsteps);
+}
+
+int mpdata_sync(mpdata_handle hh)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h) return mpd::fail(MPDATA_ERR_ARG, "null handle");
+    if (int rc = ensure_device(h)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mpdata_mass(mpdata_handle h, double* mass)
+{
+    if (!mass) return mpd::fail(MPDATA_ERR_ARG, "null output");
+    double s[3];
+    if (int rc = mpd::stats(reinterpret_cast<Solver*>(h), s)) return rc;
+    *mass = s[0];
+    return 0;
+}
+
+int mpdata_min(mpdata_handle h, double* minval, long long* nneg)
+{
+    double s[3];
+    if (int rc = mpd::stats(reinterpret_cast<Solver*>(h), s)) return rc;
+    if (minval) *minval = s[1];
+    if (nneg) *nneg = (long long)s[2];
+    return 0;
+}
+
+int mpdata_launches_per_step(mpdata_handle h)
+{
+    if (!h) return mpd::fail(MPDATA_ERR_ARG, "null handle");
+    return mpd::launches(reinterpret_cast<Solver*>(h));
+}
+
+int mpdata_enable_pass_timing(mpdata_handle hh, int on)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h) return mpd::fail(MPDATA_ERR_ARG, "null handle");
+    h->timing = on != 0;
+    return 0;
+}
+
+int mpdata_pass_times(mpdata_handle hh, double ms[3], long long launches[3], int reset)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h) return mpd::fail(MPDATA_ERR_ARG, "null handle");
+    if (int rc = ensure_device(h)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < 3; c++) {
+        for (auto& p : h->pending[c]) {
+            float t = 0;
+            CUDA_TRY(cudaEventElapsedTime(&t, p.first, p.second));
+            h->pass_ms[c] += t;
+            h->pass_n[c] += 1;
+            h->event_pool.push_back(p.first);
+            h->event_pool.push_back(p.second);
+        }
+        h->pending[c].clear();
+        if (ms) ms[c] = h->pass_ms[c];
+        if (launches) launches[c] = h->pass_n[c];
+        if (reset) {
+            h->pass_ms[c] = 0;
+            h->pass_n[c] = 0;
+        }
+    }
+    return 0;
+}
+
+void* mpdata_host_alloc(size_t bytes)
+{
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+        mpd::fail(MPDATA_ERR_NOMEM, "cudaMallocHost(%zu) failed", bytes);
+        return nullptr;
+    }
+    return p;
+}
+
+void mpdata_host_free(void* p)
+{
+    if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"

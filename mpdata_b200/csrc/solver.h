@@ -1,0 +1,57 @@
+// Internal solver state shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+#include "mpdata_b200.h"
+
+namespace mpd {
+
+struct Solver {
+    int dtype = MPDATA_F32;
+    size_t esz = 4;
+    int order = 1;
+    mpdata_options opts{};
+    Dims d{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // Field levels: c[cur] is the newest, c[prev] the level before the last pass.
+    void* c[3] = {nullptr, nullptr, nullptr};
+    int cur = 0, prev = 0;
+    // faces[0] = advective (constant between velocity updates), faces[1..2]
+    // the Jacobi ping-pong of the antidiffusive passes; [axis] = U, V, W.
+    void* faces[3][3] = {{nullptr}};
+    void* bup = nullptr;  // limiter ratios (one-kernel-per-routine path only)
+    void* bdn = nullptr;
+    void* vel[6] = {nullptr};  // velocity staging for set_velocity
+    void* metric = nullptr;    // dx | dy | ds
+    double* red = nullptr;     // reduction partials
+    bool have_field = false, have_faces = false;
+    // Optional per-pass event timing: pending event pairs per pass class.
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[3];
+    std::vector<cudaEvent_t> event_pool;
+    double pass_ms[3] = {0, 0, 0};
+    long long pass_n[3] = {0, 0, 0};
+};
+
+int fail(int code, const char* fmt, ...);
+
+int create_solver(Solver** out, int nx, int ny, int ns, int dtype, int order,
+                  const mpdata_options* opts);
+void destroy_solver(Solver* h);
+int set_velocity(Solver* h, const void* dx, const void* dy, const void* ds, double dt,
+                 const void* const vel[6], int where);
+int set_faces(Solver* h, const void* U, const void* V, const void* W, int where);
+int set_field(Solver* h, const void* c, int where);
+int get_field(Solver* h, void* c, int where, bool previous);
+int step(Solver* h, int nsteps);
+int stats(Solver* h, double out[3]);
+int launches(const Solver* h);
+
+}  // namespace mpd
