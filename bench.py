@@ -42,8 +42,16 @@ sys.path.insert(0, ROOT)
 METRIC = "Gcell-steps/s & % HBM roofline on 1 B200, plain vs chosen at stated FP64 error"
 UNIT = "Gcell-steps/s"
 NX, NY, NS, ORDER = 512, 512, 256, 3
-CELLS = (NX - 2) * (NY - 2) * (NS - 2)
-FIELD_BYTES = NX * NY * NS * 4
+
+
+def _set_size(nx, ny, ns):
+    global NX, NY, NS, CELLS, FIELD_BYTES
+    NX, NY, NS = nx, ny, ns
+    CELLS = (NX - 2) * (NY - 2) * (NS - 2)
+    FIELD_BYTES = NX * NY * NS * 4
+
+
+_set_size(NX, NY, NS)
 # Algorithmic bytes per interior cell (FP32, d = 3, IORD 3, limiter on):
 #   donor pass        reads c^n + 3 faces, writes c^(1)                      5
 #   corrective pass 1 reads c^(1), c^n, 3 faces; writes c^(2) + 3 faces      9
@@ -394,7 +402,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--size", default=None,
+                    help="nx,ny,ns override (profiling captures of a smaller grid only)")
     args = ap.parse_args()
+    if args.size:
+        _set_size(*(int(v) for v in args.size.split(",")))
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     line = run_reference(args) if args.impl == "reference" else run_gpu(args)

@@ -1,6 +1,7 @@
 // Kernel set of one arithmetic mode.  Included by kernels_fast.cu and
 // kernels_strict.cu with MPD_NS defined as the mode's namespace.
 #include "launch.h"
+#include "tma.cuh"
 
 namespace mpd {
 namespace MPD_NS {

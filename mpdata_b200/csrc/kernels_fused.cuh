@@ -1,322 +1,391 @@
 // Fused corrective pass: antidiffusive faces (+ nonoscillatory limiter) and
-// the donor-cell update of one MPDATA pass in a single kernel.
+// the donor-cell update of one MPDATA pass in one kernel, z-marching.
 //
-// Decomposition: each CTA owns a TX x TY column of interior cells and marches
-// it through z.  Per plane it stages the pass input c, the step input c^n
-// (limiter bounds) and the previous pass's faces into shared-memory rings
-// (halo 3 in x and y: the divergent term of the y faces reaches two x faces
-// back, vv.c:89, and the limiter needs the faces of the halo cells), then
-//   1. computes the new faces over the tile (+ the cells' low edge faces;
-//      with the limiter, over the tile plus a one-cell halo),
-//   2. with the limiter: the in/out ratios of every tile+halo cell,
-//   3. limits the faces of the cell it updates and applies the donor update.
-// The limiter needs the ratios of the z neighbour above, so with it the
-// update trails the face computation by one plane.
+// Work decomposition.  A CTA of 32 x 16 threads covers a 32 x 16 column of
+// cells and marches it through z.  Each thread owns one cell of the column:
+// per plane it forms the cell's three high faces (x, y and the z face above)
+// and, with the limiter, the cell's in/out ratios; then it applies the
+// donor-cell update.  Without the limiter every cell of the CTA is updated;
+// with it the outer ring of the CTA is a halo (30 x 14 cells updated) whose
+// faces and ratios the limited faces of the updated cells need.  The first
+// warps also form the faces just below the column (x face at local x = -1, y
+// face at local y = -1), which the lowest cells read.
+//
+// Staging.  The pass input c, the step input c^n (limiter bounds) and the
+// previous pass's faces U, V, W are brought in one plane at a time by TMA
+// (cp.async.bulk.tensor, 40 x 19 element boxes, zero-filled outside the grid)
+// into a four-deep ring of shared-memory stages, two planes ahead of the
+// plane being computed; one mbarrier per stage.  The box starts on a 16-byte
+// boundary in x (its low edge is rounded down and the slack is skipped).
+//
+// z dependence.  The cell's own c values of the neighbouring planes and its
+// own z faces live in registers from one plane to the next.  With the
+// limiter, the limited z face above a cell needs the ratios of the cell
+// above, so the update trails the face computation by one plane; the limited
+// x and y faces of a plane are kept (registers + a two-plane ring in shared
+// memory for the neighbours) until the update of that plane.
+//
+// Arithmetic: identical formulas and evaluation order as kernels_unfused.cuh
+// (the reference's, see there for file:line citations).
 //
 // Included by kernels_all.cuh inside namespace mpd::MPD_NS.
 
 namespace fused {
 
-constexpr int TX = 32, TY = 8, NT = TX * TY;
-constexpr int H = 3;                  // halo of every staged plane
-constexpr int SX = TX + 2 * H, SY = TY + 2 * H, PL = SX * SY;
+constexpr int BX = 32, BY = 16, NT = BX * BY;
+constexpr int SBX = kBoxX, SBY = kBoxY;      // staged plane box
+constexpr int NSTAGE = 4;
+constexpr int WX = BX + 2, WY = BY + 2, WPL = WX * WY;  // work planes: local [-1,32] x [-1,16]
 
-// Ring slots per staged array.
-constexpr int RC = 4, RCN = 4, RUO = 2, RVO = 2, RWO = 4, RRU = 2, RRV = 2, RRW = 4, RB = 4;
-
-template <bool LIM> constexpr int planes()
+template <typename T> __host__ __device__ constexpr int stage_bytes()
 {
-    return RC + RUO + RVO + RWO + RRU + RRV + RRW + (LIM ? RCN + 2 * RB : 0);
+    return (SBX * SBY * (int)sizeof(T) + 127) / 128 * 128;
+}
+template <bool LIM> __host__ __device__ constexpr int n_arrays() { return LIM ? 5 : 4; }
+template <bool LIM> __host__ __device__ constexpr int n_work() { return LIM ? 8 : 2; }
+template <typename T, bool LIM> __host__ __device__ constexpr size_t smem_bytes()
+{
+    return (size_t)NSTAGE * n_arrays<LIM>() * stage_bytes<T>() + (size_t)n_work<LIM>() * WPL * sizeof(T) +
+           NSTAGE * sizeof(uint64_t);
+}
+
+// The staged planes one face computation reads (pointers into stage slots).
+template <typename T> struct Planes {
+    const T *c_m, *c_0, *c_p;     // c at planes k-1, k, k+1
+    const T *uo_0, *uo_p;         // previous x faces, planes k, k+1
+    const T *vo_0, *vo_p;         // previous y faces, planes k, k+1
+    const T *wo_m, *wo_0, *wo_p;  // previous z faces, face-planes k-1, k, k+1
+};
+
+struct FaceCtx {
+    int nx, ny, ns, use_div, vv_fix, pass;
+};
+
+// x face between cells i and i+1 (row j, plane k); o = staged offset of cell i.
+template <typename T>
+__device__ __forceinline__ T face_u(const Planes<T>& P, int o, int i, const FaceCtx& f)
+{
+    constexpr int Y = SBX;
+    T vb, wb, neg_div = T(0);
+    if (i == 0 || i == f.nx - 2) {
+        const int a = (i == 0) ? o + 1 : o;
+        vb = T(0.5) * (P.vo_0[a - Y] + P.vo_0[a]);
+        wb = T(0.5) * (P.wo_m[a] + P.wo_0[a]);
+    } else {
+        vb = T(0.25) * (((P.vo_0[o + 1 - Y] + P.vo_0[o + 1]) + P.vo_0[o]) + P.vo_0[o - Y]);
+        wb = T(0.25) * (((P.wo_m[o + 1] + P.wo_0[o + 1]) + P.wo_0[o]) + P.wo_m[o]);
+        if (f.use_div) {
+            T s = P.uo_0[o + 1] - P.uo_0[o - 1];
+            s = s + P.vo_0[o + 1 - Y];
+            s = s - P.vo_0[o + 1];
+            s = s - P.vo_0[o];
+            s = s + P.vo_0[o - Y];
+            s = s + P.wo_m[o + 1];
+            s = s - P.wo_0[o + 1];
+            s = s - P.wo_0[o];
+            s = s + P.wo_m[o];
+            neg_div = -((T(0.25) * P.uo_0[o]) * s);
+        } else {
+            neg_div = -T(0);
+        }
+    }
+    T n1, d1, n2, d2;
+    grad_pair(P.c_0[o + 1 + Y], P.c_0[o + Y], P.c_0[o - Y], P.c_0[o + 1 - Y], n1, d1);
+    grad_pair(P.c_p[o + 1], P.c_p[o], P.c_m[o], P.c_m[o + 1], n2, d2);
+    return face_pattern(neg_div, P.uo_0[o], P.c_0[o], P.c_0[o + 1], vb, n1, d1, wb, n2, d2);
+}
+
+// y face between rows j and j+1 (column i, plane k).
+template <typename T>
+__device__ __forceinline__ T face_v(const Planes<T>& P, int o, int i, int j, int k,
+                                   const FaceCtx& f, const Dims& d, const T* __restrict__ Vadv)
+{
+    constexpr int Y = SBX;
+    T ub, wb, neg_div = T(0);
+    if (j == 0 || j == f.ny - 2) {
+        const int a = (j == 0) ? o + Y : o;
+        ub = T(0.5) * (P.uo_0[a - 1] + P.uo_0[a]);
+        wb = T(0.5) * (P.wo_m[a] + P.wo_0[a]);
+    } else {
+        if (i == 1 && !f.vv_fix)  // the column vv_pass never writes (vv.c:81-82)
+            return (f.pass & 1) ? T(0) : Vadv[cell(d, 1, j, k)];
+        ub = T(0.25) * (((P.uo_0[o - 1 + Y] + P.uo_0[o + Y]) + P.uo_0[o]) + P.uo_0[o - 1]);
+        wb = T(0.25) * (((P.wo_m[o + Y] + P.wo_0[o + Y]) + P.wo_0[o]) + P.wo_m[o]);
+        if (f.use_div) {
+            const T ul2u = (i >= 2) ? P.uo_0[o - 2 + Y] : T(0);
+            const T ul2 = (i >= 2) ? P.uo_0[o - 2] : T(0);
+            T s = P.vo_0[o + Y] - P.vo_0[o - Y];
+            s = s + P.wo_m[o + Y];
+            s = s - P.wo_0[o + Y];
+            s = s - P.wo_0[o];
+            s = s + P.wo_m[o];
+            s = s + P.uo_0[o - 1 + Y];
+            s = s - ul2u;
+            s = s - ul2;
+            s = s + P.uo_0[o - 1];
+            neg_div = -((T(0.25) * P.vo_0[o]) * s);
+        } else {
+            neg_div = -T(0);
+        }
+    }
+    T n1, d1, n2, d2;
+    grad_pair(P.c_0[o + 1 + Y], P.c_0[o + 1], P.c_0[o - 1], P.c_0[o - 1 + Y], n1, d1);
+    grad_pair(P.c_p[o + Y], P.c_p[o], P.c_m[o], P.c_m[o + Y], n2, d2);
+    return face_pattern(neg_div, P.vo_0[o], P.c_0[o], P.c_0[o + Y], ub, n1, d1, wb, n2, d2);
+}
+
+// z face between planes k and k+1 (cell column i, j).
+template <typename T>
+__device__ __forceinline__ T face_w(const Planes<T>& P, int o, int k, const FaceCtx& f)
+{
+    constexpr int Y = SBX;
+    T ub, vb, neg_div = T(0);
+    if (k == 0 || k == f.ns - 2) {
+        const T* U = (k == 0) ? P.uo_p : P.uo_0;  // the interior plane next to the face
+        const T* V = (k == 0) ? P.vo_p : P.vo_0;
+        ub = T(0.5) * (U[o - 1] + U[o]);
+        vb = T(0.5) * (V[o - Y] + V[o]);
+    } else {
+        ub = T(0.25) * (((P.uo_0[o] + P.uo_p[o]) + P.uo_p[o - 1]) + P.uo_0[o - 1]);
+        vb = T(0.25) * (((P.vo_p[o - Y] + P.vo_p[o]) + P.vo_0[o]) + P.vo_0[o - Y]);
+        if (f.use_div) {
+            T s = P.wo_p[o] - P.wo_m[o];
+            s = s + P.uo_p[o - 1];
+            s = s - P.uo_p[o];
+            s = s - P.uo_0[o];
+            s = s + P.uo_0[o - 1];
+            s = s + P.vo_p[o - Y];
+            s = s - P.vo_p[o];
+            s = s - P.vo_0[o];
+            s = s + P.vo_0[o - Y];
+            neg_div = -((T(0.25) * P.wo_0[o]) * s);
+        } else {
+            neg_div = -T(0);
+        }
+    }
+    T n1, d1, n2, d2;
+    grad_pair(P.c_p[o + 1], P.c_0[o + 1], P.c_0[o - 1], P.c_p[o - 1], n1, d1);
+    grad_pair(P.c_p[o + Y], P.c_0[o + Y], P.c_0[o - Y], P.c_p[o - Y], n2, d2);
+    return face_pattern(neg_div, P.wo_0[o], P.c_0[o], P.c_p[o], ub, n1, d1, vb, n2, d2);
 }
 
 }  // namespace fused
 
 template <typename T, bool LIM, typename A>
-__global__ void __launch_bounds__(fused::NT) k_pass_fused(Dims d, PassArgs<T> a)
+__global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
+    k_pass_tma(Dims d, PassArgs<T> a, const __grid_constant__ CUtensorMap map_c,
+               const __grid_constant__ CUtensorMap map_cn, const __grid_constant__ CUtensorMap map_uo,
+               const __grid_constant__ CUtensorMap map_vo, const __grid_constant__ CUtensorMap map_wo)
 {
     using namespace fused;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* sC = reinterpret_cast<T*>(smem_raw);
-    T* sUO = sC + RC * PL;
-    T* sVO = sUO + RUO * PL;
-    T* sWO = sVO + RVO * PL;
-    T* sRU = sWO + RWO * PL;
-    T* sRV = sRU + RRU * PL;
-    T* sRW = sRV + RRV * PL;
-    T* sCN = sRW + RRW * PL;  // limiter only
-    T* sBU = sCN + RCN * PL;
-    T* sBD = sBU + RB * PL;
+    constexpr int NARR = n_arrays<LIM>();
+    constexpr int SB = stage_bytes<T>();
+    constexpr int Y = SBX;
+    extern __shared__ __align__(128) unsigned char smem[];
+    T* work = reinterpret_cast<T*>(smem + (size_t)NSTAGE * NARR * SB);
+    T* sRU = work;              // raw x faces of plane k
+    T* sRV = sRU + WPL;         // raw y faces of plane k
+    T* sBU = sRV + WPL;         // limiter ratios of plane k
+    T* sBD = sBU + WPL;
+    T* sLU = sBD + WPL;         // limited x faces, planes k-1 / k (two slots)
+    T* sLV = sLU + 2 * WPL;     // limited y faces, two slots
+    uint64_t* bars = reinterpret_cast<uint64_t*>(work + n_work<LIM>() * WPL);
+    auto box = [&](int p, int arr) -> const T* {
+        return reinterpret_cast<const T*>(smem + (size_t)((p & (NSTAGE - 1)) * NARR + arr) * SB);
+    };
 
     const int nx = d.nx, ny = d.ny, ns = d.ns;
-    const int tid = threadIdx.y * TX + threadIdx.x;
-    const int i0 = 1 + blockIdx.x * TX, j0 = 1 + blockIdx.y * TY;
-    const int gx0 = i0 - H, gy0 = j0 - H;
+    const int x = threadIdx.x, y = threadIdx.y, tid = y * BX + x;
+    constexpr int OW = LIM ? 1 : 0;  // halo ring width
+    const int i0 = 1 + (int)blockIdx.x * (BX - 2 * OW) - OW;  // global i of local x = 0
+    const int j0 = 1 + (int)blockIdx.y * (BY - 2 * OW) - OW;
+    constexpr int ALIGN = 16 / (int)sizeof(T);                // TMA: x * size multiple of 16 B
+    const int gx0 = (i0 - 2) & ~(ALIGN - 1);
+    const int gy0 = j0 - 2;
+    const int rx = (i0 - 2) - gx0;
+    const int o = (y + 2) * Y + (x + 2 + rx);   // own cell in a staged plane
+    const int w = (y + 1) * WX + (x + 1);       // own cell in a work plane
+    const int i = i0 + x, j = j0 + y;
+    const FaceCtx fc{nx, ny, ns, a.use_div, a.vv_fix, a.pass};
+    const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
+    const bool owned = cell_in && (!LIM || (x >= 1 && x <= BX - 2 && y >= 1 && y <= BY - 2));
 
-    // Shared-memory offset of global (i, j) within a plane.
-    auto S = [&](int i, int j) { return (j - gy0) * SX + (i - gx0); };
-    auto c = [&](int p, int i, int j) { return sC[(p & (RC - 1)) * PL + S(i, j)]; };
-    auto cn = [&](int p, int i, int j) { return sCN[(p & (RCN - 1)) * PL + S(i, j)]; };
-    auto uo = [&](int p, int i, int j) { return sUO[(p & (RUO - 1)) * PL + S(i, j)]; };
-    auto vo = [&](int p, int i, int j) { return sVO[(p & (RVO - 1)) * PL + S(i, j)]; };
-    auto wo = [&](int p, int i, int j) { return sWO[(p & (RWO - 1)) * PL + S(i, j)]; };
-    auto ru = [&](int p, int i, int j) -> T& { return sRU[(p & (RRU - 1)) * PL + S(i, j)]; };
-    auto rv = [&](int p, int i, int j) -> T& { return sRV[(p & (RRV - 1)) * PL + S(i, j)]; };
-    auto rw = [&](int p, int i, int j) -> T& { return sRW[(p & (RRW - 1)) * PL + S(i, j)]; };
-    auto bu = [&](int p, int i, int j) -> T& { return sBU[(p & (RB - 1)) * PL + S(i, j)]; };
-    auto bd = [&](int p, int i, int j) -> T& { return sBD[(p & (RB - 1)) * PL + S(i, j)]; };
-    auto interior = [&](int i, int j, int p) {
-        return i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && p >= 1 && p <= ns - 2;
-    };
-
-    // Stage plane p of a full-grid array into a ring slot (zero outside the grid).
-    auto load = [&](T* ring, int slots, const T* __restrict__ src, int p) {
-        T* dst = ring + (p & (slots - 1)) * PL;
-        const T* base = src + (long long)p * d.pp;
-        for (int e = tid; e < PL; e += NT) {
-            int y = e / SX, x = e - y * SX;
-            int gi = gx0 + x, gj = gy0 + y;
-            T v = T(0);
-            if (gi >= 0 && gi < nx && gj >= 0 && gj < ny) v = base[(long long)gj * d.px + gi];
-            dst[e] = v;
-        }
-    };
-
-    // ---- face formulas (the reference's, see kernels_unfused.cuh) ----
-    auto face_u = [&](int m, int f, int j) -> T {  // x face between f and f+1, row j, plane m
-        T vb, wb, neg_div = T(0);
-        if (f == 0 || f == nx - 2) {
-            int ic = (f == 0) ? 1 : nx - 2;
-            vb = T(0.5) * (vo(m, ic, j - 1) + vo(m, ic, j));
-            wb = T(0.5) * (wo(m - 1, ic, j) + wo(m, ic, j));
-        } else {
-            vb = T(0.25) * (((vo(m, f + 1, j - 1) + vo(m, f + 1, j)) + vo(m, f, j)) + vo(m, f, j - 1));
-            wb = T(0.25) * (((wo(m - 1, f + 1, j) + wo(m, f + 1, j)) + wo(m, f, j)) + wo(m - 1, f, j));
-            if (a.use_div) {
-                T s = uo(m, f + 1, j) - uo(m, f - 1, j);
-                s = s + vo(m, f + 1, j - 1);
-                s = s - vo(m, f + 1, j);
-                s = s - vo(m, f, j);
-                s = s + vo(m, f, j - 1);
-                s = s + wo(m - 1, f + 1, j);
-                s = s - wo(m, f + 1, j);
-                s = s - wo(m, f, j);
-                s = s + wo(m - 1, f, j);
-                neg_div = -((T(0.25) * uo(m, f, j)) * s);
-            } else {
-                neg_div = -T(0);
-            }
-        }
-        T n1, d1, n2, d2;
-        grad_pair(c(m, f + 1, j + 1), c(m, f, j + 1), c(m, f, j - 1), c(m, f + 1, j - 1), n1, d1);
-        grad_pair(c(m + 1, f + 1, j), c(m + 1, f, j), c(m - 1, f, j), c(m - 1, f + 1, j), n2, d2);
-        return face_pattern(neg_div, uo(m, f, j), c(m, f, j), c(m, f + 1, j), vb, n1, d1, wb, n2, d2);
-    };
-    auto face_v = [&](int m, int i, int g) -> T {  // y face between g and g+1, column i
-        T ub, wb, neg_div = T(0);
-        if (g == 0 || g == ny - 2) {
-            int jc = (g == 0) ? 1 : ny - 2;
-            ub = T(0.5) * (uo(m, i - 1, jc) + uo(m, i, jc));
-            wb = T(0.5) * (wo(m - 1, i, jc) + wo(m, i, jc));
-        } else {
-            if (i == 1 && !a.vv_fix)  // column vv_pass never writes (vv.c:81-82)
-                return (a.pass & 1) ? T(0) : a.Vadv[cell(d, 1, g, m)];
-            ub = T(0.25) * (((uo(m, i - 1, g + 1) + uo(m, i, g + 1)) + uo(m, i, g)) + uo(m, i - 1, g));
-            wb = T(0.25) * (((wo(m - 1, i, g + 1) + wo(m, i, g + 1)) + wo(m, i, g)) + wo(m - 1, i, g));
-            if (a.use_div) {
-                T ul2u = (i >= 2) ? uo(m, i - 2, g + 1) : T(0);
-                T ul2 = (i >= 2) ? uo(m, i - 2, g) : T(0);
-                T s = vo(m, i, g + 1) - vo(m, i, g - 1);
-                s = s + wo(m - 1, i, g + 1);
-                s = s - wo(m, i, g + 1);
-                s = s - wo(m, i, g);
-                s = s + wo(m - 1, i, g);
-                s = s + uo(m, i - 1, g + 1);
-                s = s - ul2u;
-                s = s - ul2;
-                s = s + uo(m, i - 1, g);
-                neg_div = -((T(0.25) * vo(m, i, g)) * s);
-            } else {
-                neg_div = -T(0);
-            }
-        }
-        T n1, d1, n2, d2;
-        grad_pair(c(m, i + 1, g + 1), c(m, i + 1, g), c(m, i - 1, g), c(m, i - 1, g + 1), n1, d1);
-        grad_pair(c(m + 1, i, g + 1), c(m + 1, i, g), c(m - 1, i, g), c(m - 1, i, g + 1), n2, d2);
-        return face_pattern(neg_div, vo(m, i, g), c(m, i, g), c(m, i, g + 1), ub, n1, d1, wb, n2, d2);
-    };
-    auto face_w = [&](int m, int i, int j) -> T {  // z face between planes m and m+1
-        T ub, vb, neg_div = T(0);
-        if (m == 0 || m == ns - 2) {
-            int kc = (m == 0) ? 1 : ns - 2;
-            ub = T(0.5) * (uo(kc, i - 1, j) + uo(kc, i, j));
-            vb = T(0.5) * (vo(kc, i, j - 1) + vo(kc, i, j));
-        } else {
-            ub = T(0.25) * (((uo(m, i, j) + uo(m + 1, i, j)) + uo(m + 1, i - 1, j)) + uo(m, i - 1, j));
-            vb = T(0.25) * (((vo(m + 1, i, j - 1) + vo(m + 1, i, j)) + vo(m, i, j)) + vo(m, i, j - 1));
-            if (a.use_div) {
-                T s = wo(m + 1, i, j) - wo(m - 1, i, j);
-                s = s + uo(m + 1, i - 1, j);
-                s = s - uo(m + 1, i, j);
-                s = s - uo(m, i, j);
-                s = s + uo(m, i - 1, j);
-                s = s + vo(m + 1, i, j - 1);
-                s = s - vo(m + 1, i, j);
-                s = s - vo(m, i, j);
-                s = s + vo(m, i, j - 1);
-                neg_div = -((T(0.25) * wo(m, i, j)) * s);
-            } else {
-                neg_div = -T(0);
-            }
-        }
-        T n1, d1, n2, d2;
-        grad_pair(c(m + 1, i + 1, j), c(m, i + 1, j), c(m, i - 1, j), c(m + 1, i - 1, j), n1, d1);
-        grad_pair(c(m + 1, i, j + 1), c(m, i, j + 1), c(m, i, j - 1), c(m + 1, i, j - 1), n2, d2);
-        return face_pattern(neg_div, wo(m, i, j), c(m, i, j), c(m + 1, i, j), ub, n1, d1, vb, n2, d2);
-    };
-
-    // Regions (global coordinates, inclusive) over which faces are formed.
-    // Without the limiter: the tile's cells and their low edge faces; with it,
-    // every face of the tile cells and of their one-cell halo.
-    const int e = LIM ? 1 : 0;
-    const int ux0 = i0 - 1 - e, ux1 = i0 + TX - 1 + e, uy0 = j0 - e, uy1 = j0 + TY - 1 + e;
-    const int vx0 = i0 - e, vx1 = i0 + TX - 1 + e, vy0 = j0 - 1 - e, vy1 = j0 + TY - 1 + e;
-    const int wx0 = i0 - e, wx1 = i0 + TX - 1 + e, wy0 = j0 - e, wy1 = j0 + TY - 1 + e;
-
-    auto make_w = [&](int m) {  // raw z faces of face-plane m
-        const int w = wx1 - wx0 + 1, n = w * (wy1 - wy0 + 1);
-        for (int q = tid; q < n; q += NT) {
-            int y = q / w, x = q - y * w;
-            int i = wx0 + x, j = wy0 + y;
-            bool ok = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && m >= 0 && m <= ns - 2;
-            rw(m, i, j) = ok ? face_w(m, i, j) : T(0);
-        }
-    };
-    auto make_uv = [&](int m) {  // raw x and y faces of plane m
-        {
-            const int w = ux1 - ux0 + 1, n = w * (uy1 - uy0 + 1);
-            for (int q = tid; q < n; q += NT) {
-                int y = q / w, x = q - y * w;
-                int f = ux0 + x, j = uy0 + y;
-                bool ok = f >= 0 && f <= nx - 2 && j >= 1 && j <= ny - 2;
-                ru(m, f, j) = ok ? face_u(m, f, j) : T(0);
-            }
-        }
-        {
-            const int w = vx1 - vx0 + 1, n = w * (vy1 - vy0 + 1);
-            for (int q = tid; q < n; q += NT) {
-                int y = q / w, x = q - y * w;
-                int i = vx0 + x, g = vy0 + y;
-                bool ok = i >= 1 && i <= nx - 2 && g >= 0 && g <= ny - 2;
-                rv(m, i, g) = ok ? face_v(m, i, g) : T(0);
-            }
-        }
-    };
-    auto make_beta = [&](int m) {  // limiter ratios of the tile + halo cells of plane m
-        const int w = TX + 2, n = w * (TY + 2);
-        for (int q = tid; q < n; q += NT) {
-            int y = q / w, x = q - y * w;
-            int i = i0 - 1 + x, j = j0 - 1 + y;
-            if (!interior(i, j, m)) { bu(m, i, j) = T(1); bd(m, i, j) = T(1); continue; }
-            T psi = c(m, i, j), mx = psi, mn = psi, t;
-#define MPD_BOUND(v) do { t = (v); mx = t > mx ? t : mx; mn = t < mn ? t : mn; } while (0)
-            MPD_BOUND(cn(m, i, j));
-            MPD_BOUND(c(m, i - 1, j)); MPD_BOUND(cn(m, i - 1, j));
-            MPD_BOUND(c(m, i + 1, j)); MPD_BOUND(cn(m, i + 1, j));
-            MPD_BOUND(c(m, i, j - 1)); MPD_BOUND(cn(m, i, j - 1));
-            MPD_BOUND(c(m, i, j + 1)); MPD_BOUND(cn(m, i, j + 1));
-            if (ns > 3) {
-                MPD_BOUND(c(m - 1, i, j)); MPD_BOUND(cn(m - 1, i, j));
-                MPD_BOUND(c(m + 1, i, j)); MPD_BOUND(cn(m + 1, i, j));
-            }
-#undef MPD_BOUND
-            A fin = A(0), fout = A(0);
-            lim_acc(lim_flux<T, A>(ru(m, i - 1, j), c(m, i - 1, j), psi), false, fin, fout);
-            lim_acc(lim_flux<T, A>(ru(m, i, j), psi, c(m, i + 1, j)), true, fin, fout);
-            lim_acc(lim_flux<T, A>(rv(m, i, j - 1), c(m, i, j - 1), psi), false, fin, fout);
-            lim_acc(lim_flux<T, A>(rv(m, i, j), psi, c(m, i, j + 1)), true, fin, fout);
-            lim_acc(lim_flux<T, A>(rw(m - 1, i, j), c(m - 1, i, j), psi), false, fin, fout);
-            lim_acc(lim_flux<T, A>(rw(m, i, j), psi, c(m + 1, i, j)), true, fin, fout);
-            bu(m, i, j) = T((A(mx) - A(psi)) / (fin + lim_tiny<A>()));
-            bd(m, i, j) = T((A(psi) - A(mn)) / (fout + lim_tiny<A>()));
-        }
-    };
-    // Ratio of cell (i, j, p), 1 for the fixed shell.
-    auto BU = [&](int p, int i, int j) { return interior(i, j, p) ? bu(p, i, j) : T(1); };
-    auto BD = [&](int p, int i, int j) { return interior(i, j, p) ? bd(p, i, j) : T(1); };
-    auto FU = [&](int p, int f, int j) {
-        T r = ru(p, f, j);
-        if (!LIM) return r;
-        return limit_face(r, BU(p, f, j), BD(p, f, j), BU(p, f + 1, j), BD(p, f + 1, j));
-    };
-    auto FV = [&](int p, int i, int g) {
-        T r = rv(p, i, g);
-        if (!LIM) return r;
-        return limit_face(r, BU(p, i, g), BD(p, i, g), BU(p, i, g + 1), BD(p, i, g + 1));
-    };
-    auto FW = [&](int q, int i, int j) {  // face-plane q
-        T r = rw(q, i, j);
-        if (!LIM) return r;
-        return limit_face(r, BU(q, i, j), BD(q, i, j), BU(q + 1, i, j), BD(q + 1, i, j));
-    };
-
-    // ---- prologue: planes 0 and 1, z faces of face-plane 0 ----
-    load(sC, RC, a.c, 0);
-    load(sC, RC, a.c, 1);
-    if (LIM) {
-        load(sCN, RCN, a.cn, 0);
-        load(sCN, RCN, a.cn, 1);
+    if (tid == 0) {
+        for (int s = 0; s < NSTAGE; s++) tma::mbar_init(&bars[s], 1);
+        tma::fence_barrier_init();
+        tma::prefetch_map(&map_c);
+        tma::prefetch_map(&map_uo);
+        tma::prefetch_map(&map_vo);
+        tma::prefetch_map(&map_wo);
+        if (LIM) tma::prefetch_map(&map_cn);
     }
-    load(sUO, RUO, a.Uo, 1);
-    load(sVO, RVO, a.Vo, 1);
-    load(sWO, RWO, a.Wo, 0);
-    load(sWO, RWO, a.Wo, 1);
     __syncthreads();
-    make_w(0);
 
-    const int my_i = i0 + threadIdx.x, my_j = j0 + threadIdx.y;
-    const bool mine = my_i <= nx - 2 && my_j <= ny - 2;
+    auto issue = [&](int p) {  // one elected thread: stage plane p of every array
+        uint64_t* bar = &bars[p & (NSTAGE - 1)];
+        tma::fence_proxy_async_shared();
+        tma::mbar_arrive_expect_tx(bar, (uint32_t)(NARR * SBX * SBY * sizeof(T)));
+        T* dst = const_cast<T*>(box(p, 0));
+        tma::load_3d(dst, &map_c, gx0, gy0, p, bar);
+        tma::load_3d(const_cast<T*>(box(p, 1)), &map_uo, gx0, gy0, p, bar);
+        tma::load_3d(const_cast<T*>(box(p, 2)), &map_vo, gx0, gy0, p, bar);
+        tma::load_3d(const_cast<T*>(box(p, 3)), &map_wo, gx0, gy0, p, bar);
+        if (LIM) tma::load_3d(const_cast<T*>(box(p, 4)), &map_cn, gx0, gy0, p, bar);
+    };
+    auto planes = [&](int k) {
+        Planes<T> P;
+        P.c_m = box(k - 1, 0); P.c_0 = box(k, 0); P.c_p = box(k + 1, 0);
+        P.uo_0 = box(k, 1); P.uo_p = box(k + 1, 1);
+        P.vo_0 = box(k, 2); P.vo_p = box(k + 1, 2);
+        P.wo_m = box(k - 1, 3); P.wo_0 = box(k, 3); P.wo_p = box(k + 1, 3);
+        return P;
+    };
+
+    bool ok = true;
+    int confirmed = 0;  // planes whose stage thread 0 has seen complete
+    if (tid == 0) {
+        issue(0);
+        issue(1);
+    }
+    ok = tma::mbar_wait(&bars[0], 0);
+    if (tid == 0 && ok) confirmed = 1;
+
+    // Register state carried between planes.
+    T cq0 = T(0), cq1 = T(0), cq2 = ok ? box(0, 0)[o] : T(0), cq3 = T(0);  // own c, planes k-2..k+1
+    T rw_prev = T(0);                      // raw z face below (face-plane k-1)
+    T bu_prev = T(1), bd_prev = T(1);      // own ratios of plane k-1
+    T lu_prev = T(0), lv_prev = T(0), lw_prev = T(0);  // limited faces of plane k-1 / face-plane k-2
+
     const int last = LIM ? ns - 1 : ns - 2;
-    for (int m = 1; m <= last; m++) {
-        __syncthreads();  // ring slots of plane m+1 are free again
-        if (m + 1 <= ns - 1) {
-            load(sC, RC, a.c, m + 1);
-            if (LIM) load(sCN, RCN, a.cn, m + 1);
+    for (int k = 0; k <= last; k++) {
+        __syncthreads();  // every read of the slot plane k+2 reuses is done
+        if (tid == 0 && k + 2 <= ns - 1) issue(k + 2);
+        if (k + 1 <= ns - 1) {
+            if (ok) ok = tma::mbar_wait(&bars[(k + 1) & (NSTAGE - 1)], ((k + 1) / NSTAGE) & 1);
+            if (tid == 0 && ok) confirmed = k + 2;
+            cq3 = box(k + 1, 0)[o];
         }
-        if (m + 1 <= ns - 2) {
-            load(sUO, RUO, a.Uo, m + 1);
-            load(sVO, RVO, a.Vo, m + 1);
-            load(sWO, RWO, a.Wo, m + 1);
-        }
-        __syncthreads();
-        if (m <= ns - 2) {
-            make_uv(m);
-            make_w(m);
-            if (LIM) {
-                __syncthreads();
-                make_beta(m);
+        const bool kin = k >= 1 && k <= ns - 2;
+
+        // ---- raw faces of plane k (z face: face-plane k) ----
+        T ru = T(0), rv = T(0), rw = T(0);
+        if (k <= ns - 2) {
+            const Planes<T> P = planes(k);
+            if (kin && i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2) ru = face_u(P, o, i, fc);
+            if (kin && i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2)
+                rv = face_v(P, o, i, j, k, fc, d, a.Vadv);
+            if (cell_in) rw = face_w(P, o, k, fc);
+            sRU[w] = ru;
+            sRV[w] = rv;
+            if (tid < BY) {  // x faces just left of the column
+                const int ye = tid, ie = i0 - 1, je = j0 + ye;
+                T v = T(0);
+                if (kin && ie >= 0 && ie <= nx - 2 && je >= 1 && je <= ny - 2)
+                    v = face_u(P, (ye + 2) * Y + (1 + rx), ie, fc);
+                sRU[(ye + 1) * WX] = v;
+            } else if (tid < BY + BX) {  // y faces just below the column
+                const int xe = tid - BY, ie = i0 + xe, je = j0 - 1;
+                T v = T(0);
+                if (kin && ie >= 1 && ie <= nx - 2 && je >= 0 && je <= ny - 2)
+                    v = face_v(P, Y + (xe + 2 + rx), ie, je, k, fc, d, a.Vadv);
+                sRV[xe + 1] = v;
             }
         }
         __syncthreads();
-        const int u = LIM ? m - 1 : m;  // plane updated this iteration
-        if (u >= 1 && mine) {
-            const int i = my_i, j = my_j;
-            T ur = FU(u, i, j), ul = FU(u, i - 1, j);
-            T vt = FV(u, i, j), vb = FV(u, i, j - 1);
-            T wf = FW(u, i, j), wb = FW(u - 1, i, j);
-            T out = donor_update(c(u, i, j), c(u, i - 1, j), c(u, i + 1, j), c(u, i, j - 1),
-                                 c(u, i, j + 1), c(u - 1, i, j), c(u + 1, i, j), ur, ul, vt, vb,
-                                 wf, wb);
-            const long long q = cell(d, i, j, u);
-            a.c_out[q] = out;
+
+        if (LIM) {
+            // ---- limiter ratios of plane k ----
+            T bu = T(1), bd = T(1);
+            if (kin && cell_in) {
+                const T* c0 = box(k, 0);
+                const T* n0 = box(k, 4);
+                const T psi = cq2;
+                T mx = psi, mn = psi, t;
+#define MPD_BOUND(v) do { t = (v); mx = t > mx ? t : mx; mn = t < mn ? t : mn; } while (0)
+                MPD_BOUND(n0[o]);
+                MPD_BOUND(c0[o - 1]); MPD_BOUND(n0[o - 1]);
+                MPD_BOUND(c0[o + 1]); MPD_BOUND(n0[o + 1]);
+                MPD_BOUND(c0[o - Y]); MPD_BOUND(n0[o - Y]);
+                MPD_BOUND(c0[o + Y]); MPD_BOUND(n0[o + Y]);
+                if (ns > 3) {
+                    MPD_BOUND(cq1); MPD_BOUND(box(k - 1, 4)[o]);
+                    MPD_BOUND(cq3); MPD_BOUND(box(k + 1, 4)[o]);
+                }
+#undef MPD_BOUND
+                A fin = A(0), fout = A(0);
+                lim_acc(lim_flux<T, A>(sRU[w - 1], c0[o - 1], psi), false, fin, fout);
+                lim_acc(lim_flux<T, A>(ru, psi, c0[o + 1]), true, fin, fout);
+                lim_acc(lim_flux<T, A>(sRV[w - WX], c0[o - Y], psi), false, fin, fout);
+                lim_acc(lim_flux<T, A>(rv, psi, c0[o + Y]), true, fin, fout);
+                lim_acc(lim_flux<T, A>(rw_prev, cq1, psi), false, fin, fout);
+                lim_acc(lim_flux<T, A>(rw, psi, cq3), true, fin, fout);
+                bu = T((A(mx) - A(psi)) / (fin + lim_tiny<A>()));
+                bd = T((A(psi) - A(mn)) / (fout + lim_tiny<A>()));
+            }
+            sBU[w] = bu;
+            sBD[w] = bd;
+            __syncthreads();
+
+            // ---- limited faces: x, y of plane k; z of face-plane k-1 ----
+            T lu = ru, lv = rv;
+            if (x < BX - 1) lu = limit_face(ru, bu, bd, sBU[w + 1], sBD[w + 1]);
+            if (y < BY - 1) lv = limit_face(rv, bu, bd, sBU[w + WX], sBD[w + WX]);
+            const T lw = limit_face(rw_prev, bu_prev, bd_prev, bu, bd);
+            sLU[(k & 1) * WPL + w] = lu;
+            sLV[(k & 1) * WPL + w] = lv;
             if (a.write_faces) {
-                a.Un[q] = ur;
-                a.Vn[q] = vt;
-                a.Wn[q] = wf;
-                if (i == 1) a.Un[q - 1] = ul;
-                if (j == 1) a.Vn[q - d.px] = vb;
-                if (u == 1) a.Wn[q - d.pp] = wb;
+                const bool ox = x >= 1 && x <= BX - 2, oy = y >= 1 && y <= BY - 2;
+                const long long q = cell(d, i, j, k);
+                if (kin && i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2 && oy && (ox || i == 0))
+                    a.Un[q] = lu;
+                if (kin && i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2 && ox && (oy || j == 0))
+                    a.Vn[q] = lv;
+                if (k >= 1 && owned) a.Wn[q - d.pp] = lw;
+            }
+
+            // ---- donor update of plane k-1 ----
+            const int u = k - 1;
+            if (u >= 1 && u <= ns - 2 && owned) {
+                const T* cu = box(u, 0);
+                const T ul = sLU[(u & 1) * WPL + w - 1];
+                const T vb = sLV[(u & 1) * WPL + w - WX];
+                a.c_out[cell(d, i, j, u)] =
+                    donor_update(cu[o], cu[o - 1], cu[o + 1], cu[o - Y], cu[o + Y], cq0, cq2, lu_prev,
+                                 ul, lv_prev, vb, lw, lw_prev);
+            }
+            lu_prev = lu;
+            lv_prev = lv;
+            lw_prev = lw;
+            bu_prev = bu;
+            bd_prev = bd;
+        } else {
+            // ---- donor update of plane k ----
+            if (kin && owned) {
+                const T* c0 = box(k, 0);
+                const T ul = sRU[w - 1], vb = sRV[w - WX];
+                const long long q = cell(d, i, j, k);
+                a.c_out[q] = donor_update(c0[o], c0[o - 1], c0[o + 1], c0[o - Y], c0[o + Y], cq1,
+                                          cq3, ru, ul, rv, vb, rw, rw_prev);
+                if (a.write_faces) {
+                    a.Un[q] = ru;
+                    a.Vn[q] = rv;
+                    a.Wn[q] = rw;
+                    if (i == 1) a.Un[q - 1] = ul;
+                    if (j == 1) a.Vn[q - d.px] = vb;
+                    if (k == 1) a.Wn[q - d.pp] = rw_prev;
+                }
             }
         }
+        rw_prev = rw;
+        cq0 = cq1;
+        cq1 = cq2;
+        cq2 = cq3;
+    }
+
+    if (!ok && a.err) atomicOr(a.err, 1);
+    if (tid == 0) {  // never leave with a copy in flight
+        for (int p = confirmed; p <= ns - 1 && p <= last + 1; p++)
+            if (!tma::mbar_wait(&bars[p & (NSTAGE - 1)], (p / NSTAGE) & 1)) break;
     }
 }
 
@@ -324,15 +393,19 @@ template <typename T, bool LIM, typename A>
 int launch_fused_variant(const Dims& d, const PassArgs<T>& a, cudaStream_t s)
 {
     using namespace fused;
-    const size_t smem = (size_t)planes<LIM>() * PL * sizeof(T);
-    static bool configured = false;  // per instantiation; attribute is per device function
+    constexpr size_t smem = smem_bytes<T, LIM>();
+    static bool configured = false;  // the attribute is per device function
     if (!configured) {
-        cudaFuncSetAttribute(k_pass_fused<T, LIM, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_pass_tma<T, LIM, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         configured = true;
     }
-    dim3 g((d.nx - 2 + TX - 1) / TX, (d.ny - 2 + TY - 1) / TY), b(TX, TY);
-    k_pass_fused<T, LIM, A><<<g, b, smem, s>>>(d, a);
+    constexpr int OW = LIM ? 1 : 0;
+    dim3 g((d.nx - 2 + BX - 2 * OW - 1) / (BX - 2 * OW), (d.ny - 2 + BY - 2 * OW - 1) / (BY - 2 * OW));
+    dim3 b(BX, BY);
+    const CUtensorMap& cn = LIM ? *a.maps.cn : *a.maps.c;
+    k_pass_tma<T, LIM, A><<<g, b, smem, s>>>(d, a, *a.maps.c, cn, *a.maps.uo, *a.maps.vo,
+                                             *a.maps.wo);
     return 1;
 }
 

@@ -4,14 +4,32 @@
 // reference arithmetic).  Both expose the same launcher set.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
 
 namespace mpd {
 
+// TMA descriptors of the arrays a fused pass stages (host-side copies; the
+// launcher passes them to the kernel by value).
+struct PassMaps {
+    const CUtensorMap* c;
+    const CUtensorMap* cn;
+    const CUtensorMap* uo;
+    const CUtensorMap* vo;
+    const CUtensorMap* wo;
+};
+
+// Box staged per plane by the fused kernels: 40 x 19 elements (x: two halo
+// columns below, up to three columns of 16-byte alignment slack, 32 + 1
+// above; y: two halo rows below, 16 + 1 above).
+constexpr int kBoxX = 40, kBoxY = 19;
+
 // Per-pass description for the corrective-pass launchers.
 template <typename T> struct PassArgs {
+    PassMaps maps;     // fused path: descriptors of c, cn, Uo, Vo, Wo
+    int* err;          // device error word (bounded-wait timeouts); may be null
     const T* c;        // this pass's input field (level o)
     const T* cn;       // the step's input field (limiter bounds); may be null without limiter
     const T* Uo;       // previous pass's faces (advective on pass 1)

@@ -86,7 +86,7 @@ template <typename T> int smolar_host(int nx, int ny, int ns, T* dx, T* dy, T* d
     T* other = (order & 1) ? *c0 : *c1;
     if (int rc = mpd::get_field(h, newest, MPDATA_HOST, false)) return rc;
     if (int rc = mpd::get_field(h, other, MPDATA_HOST, true)) return rc;
-    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (int rc = mpd::check_device_error(h)) return rc;
     *c1 = newest;
     *c0 = other;
     return 0;
@@ -282,8 +282,10 @@ template <typename T> int msmolar_gather_host(void** desc, T** c0, T** c1)
                                (size_t)g->d.ny * g->d.ns, cudaMemcpyDeviceToHost, g->stream));
     CUDA_TRY(cudaMemcpy2DAsync(*c0, w, g->c[D->prev], (size_t)g->d.px * g->esz, w,
                                (size_t)g->d.ny * g->d.ns, cudaMemcpyDeviceToHost, g->stream));
-    CUDA_TRY(cudaStreamSynchronize(g->stream));
-    return 0;
+    for (Block& b : D->blocks)
+        if (b.s)
+            if (int rc = mpd::check_device_error(b.s)) return rc;
+    return mpd::check_device_error(g);
 }
 
 }  // namespace

@@ -284,6 +284,8 @@ template <typename T> int step_impl(Solver* h, int nsteps)
             const int rs = (o == 1) ? 0 : 1 + ((o - 2) & 1);
             const int ws = 1 + ((o - 1) & 1);
             mpd::PassArgs<T> a;
+            a.maps = {&h->tm_c[in], &h->tm_c[b0], &h->tm_f[rs][0], &h->tm_f[rs][1], &h->tm_f[rs][2]};
+            a.err = h->dev_err;
             a.c = Cb<T>(h, in);
             a.cn = Cb<T>(h, b0);
             a.Uo = F<T>(h, rs, 0);
@@ -324,12 +326,59 @@ template <typename T> int launches_per_step(const Solver* h)
     return n;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// Descriptor of one full-grid array for the fused kernels' per-plane boxes.
+int make_map(const Solver* h, void* ptr, CUtensorMap* map)
+{
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return mpd::fail(MPDATA_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[3] = {(cuuint64_t)h->d.nx, (cuuint64_t)h->d.ny, (cuuint64_t)h->d.ns};
+    cuuint64_t strides[2] = {(cuuint64_t)(h->d.px * h->esz), (cuuint64_t)(h->d.pp * h->esz)};
+    cuuint32_t box[3] = {(cuuint32_t)mpd::kBoxX, (cuuint32_t)mpd::kBoxY, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(map, h->dtype == MPDATA_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                                 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                     3, ptr, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return mpd::fail(MPDATA_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return 0;
+}
+
 int alloc_solver(Solver* h)
 {
     size_t fb = field_bytes(h);
     for (int b = 0; b < 3; b++) CUDA_TRY(cudaMalloc(&h->c[b], fb));
     for (int s = 0; s < 3; s++)
         for (int a = 0; a < 3; a++) CUDA_TRY(cudaMalloc(&h->faces[s][a], fb));
+    CUDA_TRY(cudaMalloc(&h->dev_err, sizeof(int)));
+    CUDA_TRY(cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream));
+    if (h->opts.kernel == 0) {
+        for (int b = 0; b < 3; b++)
+            if (int rc = make_map(h, h->c[b], &h->tm_c[b])) return rc;
+        for (int s = 0; s < 3; s++)
+            for (int a = 0; a < 3; a++)
+                if (int rc = make_map(h, h->faces[s][a], &h->tm_f[s][a])) return rc;
+    }
     if (h->opts.kernel != 0 && h->opts.limiter) {
         CUDA_TRY(cudaMalloc(&h->bup, fb));
         CUDA_TRY(cudaMalloc(&h->bdn, fb));
@@ -359,6 +408,7 @@ void free_solver(Solver* h)
     cudaFree(h->bdn);
     cudaFree(h->red);
     cudaFree(h->metric);
+    cudaFree(h->dev_err);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -518,6 +568,18 @@ int mpd::stats(Solver* h, double out[3])
     CUDA_TRY(cudaMemcpyAsync(out, h->red + 4 * mpd::kRedBlocks, 3 * sizeof(double),
                              cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return check_device_error(h);
+}
+
+int mpd::check_device_error(Solver* h)
+{
+    int flag = 0;
+    CUDA_TRY(cudaMemcpyAsync(&flag, h->dev_err, sizeof flag, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (flag) {
+        CUDA_TRY(cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream));
+        return fail(MPDATA_ERR_CUDA, "fused pass: a staged-plane wait timed out (results invalid)");
+    }
     return 0;
 }
 
@@ -603,7 +665,8 @@ int mpdata_sync(mpdata_handle hh)
     if (!h) return mpd::fail(MPDATA_ERR_ARG, "null handle");
     if (int rc = ensure_device(h)) return rc;
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return 0;
+    CUDA_TRY(cudaGetLastError());
+    return mpd::check_device_error(h);
 }
 
 int mpdata_mass(mpdata_handle h, double* mass)

@@ -1,6 +1,7 @@
 // Internal solver state shared by the C-ABI translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <utility>
@@ -31,6 +32,10 @@ struct Solver {
     void* vel[6] = {nullptr};  // velocity staging for set_velocity
     void* metric = nullptr;    // dx | dy | ds
     double* red = nullptr;     // reduction partials
+    int* dev_err = nullptr;    // device error word (bounded-wait timeouts in the fused pass)
+    // TMA descriptors of the three field levels and the nine face arrays.
+    CUtensorMap tm_c[3];
+    CUtensorMap tm_f[3][3];
     bool have_field = false, have_faces = false;
     // Optional per-pass event timing: pending event pairs per pass class.
     bool timing = false;
@@ -52,6 +57,7 @@ int set_field(Solver* h, const void* c, int where);
 int get_field(Solver* h, void* c, int where, bool previous);
 int step(Solver* h, int nsteps);
 int stats(Solver* h, double out[3]);
+int check_device_error(Solver* h);  // synchronises; reports a kernel's recorded error
 int launches(const Solver* h);
 
 }  // namespace mpd
