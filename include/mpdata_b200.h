@@ -189,6 +189,29 @@ int mpdata_launches_per_step(mpdata_handle h);
 int mpdata_enable_pass_timing(mpdata_handle h, int on);
 int mpdata_pass_times(mpdata_handle h, double ms[3], long long launches[3], int reset);
 
+/* ---- 3. Allocation-free step --------------------------------------------
+ *
+ * No counterpart in the reference.  One FP32 step (`order` passes, optional
+ * limiter, reference arithmetic, default FMA contraction) from advective faces
+ * U, V, W and the field c_in to c_out, all caller-owned DEVICE arrays in the
+ * dense full-grid layout (faces as for mpdata_set_faces), queued on `stream`
+ * (a cudaStream_t; NULL = legacy default stream).  For callers that cannot
+ * allocate device memory while they run (inside stream capture, under a
+ * fixed memory budget, inside a host framework that owns the allocator): it
+ * calls no cudaMalloc/cudaFree and no allocating library routine.  Its
+ * intermediate levels, pseudo-velocity faces and limiter ratios live in one
+ * static device array of MPDATA_NOALLOC_MAX_FLOATS floats (32 MiB, held by
+ * every GPU that loads the library until exit); grids needing more
+ * (10 * nx*ny*ns floats, i.e. more than 838860 cells) are rejected with
+ * MPDATA_ERR_ARG.  All calls share that array: calls that overlap on the GPU
+ * race, so keep them on one stream.  The first call on each device looks up
+ * the array's address (and may load the module): make it before any stream
+ * capture.  c_out must not alias c_in. */
+#define MPDATA_NOALLOC_MAX_FLOATS (8u << 20)
+int mpdata_step_noalloc(int nx, int ny, int ns, int order, int limiter, const float* U,
+                        const float* V, const float* W, const float* c_in, float* c_out,
+                        void* stream);
+
 /* Page-locked host memory for fast staging (cudaMallocHost / cudaFreeHost). */
 void* mpdata_host_alloc(size_t bytes);
 void mpdata_host_free(void* p);
