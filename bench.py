@@ -59,6 +59,11 @@ _set_size(NX, NY, NS)
 B_DONOR, B_CORR_FACES, B_CORR_LAST = 5 * 4, 9 * 4, 6 * 4
 B_STEP = B_DONOR + B_CORR_FACES + B_CORR_LAST  # 80 B per cell-step
 FALLBACK_HBM_GBS = 6650.0
+# Arithmetic forms timed ("plain" = IEEE FP32 throughout); the headline value is
+# the fastest form whose result stays within the FP64 error bound.
+FORMS = [("plain", {}), ("precision_form", {"precision_form": True}),
+         ("approx_div", {"approx_div": True})]
+FP64_REL_L2_BOUND = 1e-5
 CONFIG_TEXT = "roofline: 512x512x256 FP32, IORD 3 + nonoscillatory limiter, streamfunction flow"
 
 
@@ -248,45 +253,74 @@ def run_gpu(args):
                                 device_id=torch.device("cuda", local))
     wl = _workload()
     stream = torch.cuda.current_stream()
-    s = m.Solver(NX, NY, NS, order=ORDER, limiter=True)
-    s.set_stream(stream.cuda_stream)
-    s.set_faces(wl["U"], wl["V"], wl["W"])
-    s.set_field(wl["c0"])
-    s.step(args.warmup)
-    torch.cuda.synchronize()
-    s.enable_pass_timing(True)
-    s.pass_times(reset=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        s.step(1)
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    t_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-        dist.barrier()
-    ms, n = s.pass_times()
-    s.enable_pass_timing(False)
-    mn, nneg = s.min()
-    launches = s.launches_per_step() * args.steps
-    value = world * CELLS * args.steps / (t_ms * 1e-3) / 1e9
+
+    def timed_form(opts):
+        """W untimed steps, then EXACTLY K timed steps of one arithmetic form."""
+        s = m.Solver(NX, NY, NS, order=ORDER, limiter=True, **opts)
+        s.set_stream(stream.cuda_stream)
+        s.set_faces(wl["U"], wl["V"], wl["W"])
+        s.set_field(wl["c0"])
+        s.step(args.warmup)
+        torch.cuda.synchronize()
+        s.enable_pass_timing(True)
+        s.pass_times(reset=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            s.step(1)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        t_ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([t_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_ms = float(t.item())
+            dist.barrier()
+        ms, n = s.pass_times()
+        s.enable_pass_timing(False)
+        mn, nneg = s.min()
+        r = dict(t_ms=t_ms, ms=ms, n=n, min=mn, nneg=nneg, clk=clk,
+                 launches=s.launches_per_step() * args.steps, final=s.get_field())
+        s.close()
+        return r
+
+    results = {name: timed_form(o) for name, o in FORMS}
+    # FP64 run of the plain method over the same W + K steps: the error each
+    # FP32 form is stated against.
+    s64 = m.Solver(NX, NY, NS, order=ORDER, dtype=np.float64, limiter=True)
+    s64.set_stream(stream.cuda_stream)
+    s64.set_faces(*(wl[k].astype(np.float64) for k in ("U", "V", "W")))
+    s64.set_field(wl["c0"].astype(np.float64))
+    s64.step(args.warmup + args.steps)
+    ref64 = s64.get_field()
+    s64.close()
+    nref = float(np.linalg.norm(ref64))
+    forms = {}
+    for name, r in results.items():
+        diff = r.pop("final").astype(np.float64) - ref64
+        r["rel_l2_vs_fp64"] = float(np.linalg.norm(diff)) / nref
+        r["max_abs_vs_fp64"] = float(np.abs(diff).max())
+        r["value"] = world * CELLS * args.steps / (r["t_ms"] * 1e-3) / 1e9
+        forms[name] = r
+    del ref64
+    ok_forms = [k for k, r in forms.items() if r["rel_l2_vs_fp64"] <= FP64_REL_L2_BOUND and r["nneg"] == 0]
+    chosen = max(ok_forms, key=lambda k: forms[k]["value"]) if ok_forms else "plain"
+    sel = forms[chosen]
+    t_ms, ms, n, clk = sel["t_ms"], sel["ms"], sel["n"], sel["clk"]
+    mn, nneg, launches, value = sel["min"], sel["nneg"], sel["launches"], sel["value"]
 
     # e2e through the reference-facing smolar() with pinned host buffers
     e2e = None
     if rank == 0 and not args.no_e2e:
-        e2e = run_e2e(m, args)
-    s.close()
+        e2e = run_e2e(m, args, dict(FORMS)[chosen])
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -320,7 +354,14 @@ def run_gpu(args):
                               "frac": step_gbs / peak}},
         "gpu_launches": launches,
         "positivity": {"min": mn, "negative_cells": nneg},
+        "form": chosen,
+        "forms": {k: {"value": r["value"], "ms_per_step": r["t_ms"] / args.steps,
+                      "rel_l2_vs_fp64": r["rel_l2_vs_fp64"], "max_abs_vs_fp64": r["max_abs_vs_fp64"],
+                      "negative_cells": r["nneg"], "options": dict(FORMS)[k]}
+                  for k, r in forms.items()},
     }
+    line["config"]["form"] = chosen
+    line["config"]["fp64_error_bound"] = f"relative L2 <= {FP64_REL_L2_BOUND} and no negative cell"
     if clk:
         line["clocks"] = clk
     if e2e:
@@ -332,7 +373,7 @@ def run_gpu(args):
     return line
 
 
-def run_e2e(m, args):
+def run_e2e(m, args, form_opts):
     """Same workload through smolar() (the drop-in entry point) with pinned
     host arrays; per step: upload of the 3 distinct velocity arrays + field,
     download of the newest field and the previous level."""
@@ -352,7 +393,7 @@ def run_e2e(m, args):
     bufs = [pinned(x) for x in (u, v, w, wl["c0"], np.zeros_like(wl["c0"]))]
     hu, hv, hw, c0, c1 = (b for b, _ in bufs)
     dx = np.ones(NX, np.float32); dy = np.ones(NY, np.float32); ds = np.ones(NS, np.float32)
-    m.set_default_options(m.SolverOptions(limiter=True))
+    m.set_default_options(m.SolverOptions(limiter=True, **form_opts))
     steps = max(1, min(args.steps, args.e2e_steps))
     try:
         for it in range(2 + steps):

@@ -132,6 +132,9 @@ typedef struct mpdata_options {
     int kernel;         /* 0: fused per-pass kernels (default); 1: one kernel per
                            reference function (slower; cross-check path) */
     int check_courant;  /* 1: reject advective faces with |Courant| > 1 */
+    int approx_div;     /* 1 (F32, fused kernels, not strict): the ratios of the
+                           antidiffusive velocity and of the limiter use the
+                           hardware reciprocal (<= 2 ulp) instead of IEEE division */
 } mpdata_options;
 
 /* Fill *o with the defaults (all zero: reference behaviour, fused kernels). */

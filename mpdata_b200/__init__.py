@@ -54,7 +54,7 @@ class Options(C.Structure):
     """struct mpdata_options (include/mpdata_b200.h)."""
     _fields_ = [("limiter", C.c_int), ("precision_form", C.c_int), ("div_mode", C.c_int),
                 ("vv_fix", C.c_int), ("strict", C.c_int), ("kernel", C.c_int),
-                ("check_courant", C.c_int)]
+                ("check_courant", C.c_int), ("approx_div", C.c_int)]
 
 
 _vp = C.c_void_p
@@ -228,11 +228,12 @@ class SolverOptions:
     strict: bool = False
     kernel: int = 0  # 0 fused per-pass kernels, 1 one kernel per reference routine
     check_courant: bool = False
+    approx_div: bool = False
 
     def to_c(self) -> Options:
         return Options(int(self.limiter), int(self.precision_form), int(self.div_mode),
                        int(self.vv_fix), int(self.strict), int(self.kernel),
-                       int(self.check_courant))
+                       int(self.check_courant), int(self.approx_div))
 
 
 class Solver:

@@ -18,15 +18,18 @@
 // plane being computed; one mbarrier per stage.  The box starts on a 16-byte
 // boundary in x (its low edge is rounded down and the slack is skipped).
 //
-// z dependence.  The cell's own c values of the neighbouring planes and its
-// own z faces live in registers from one plane to the next.  With the
-// limiter, the limited z face above a cell needs the ratios of the cell
-// above, so the update trails the face computation by one plane; the limited
-// x and y faces of a plane are kept (registers + a two-plane ring in shared
-// memory for the neighbours) until the update of that plane.
+// Per plane each thread reads the 39 staged values its three faces use once
+// into registers (struct Nb) and evaluates every formula from them.  The
+// cell's own c values of the neighbouring planes and its own z faces live in
+// registers from one plane to the next.  With the limiter, the limited z face
+// above a cell needs the ratios of the cell above, so the update trails the
+// face computation by one plane; the limited x and y faces of a plane are
+// kept (registers + a two-plane ring in shared memory for the neighbours)
+// until the update of that plane.
 //
-// Arithmetic: identical formulas and evaluation order as kernels_unfused.cuh
-// (the reference's, see there for file:line citations).
+// Arithmetic: the formulas and evaluation order of kernels_unfused.cuh (the
+// reference's, see there for file:line citations).  APPROX replaces the
+// ratios' IEEE divisions by the hardware reciprocal (the "approx_div" form).
 //
 // Included by kernels_all.cuh inside namespace mpd::MPD_NS.
 
@@ -57,121 +60,163 @@ template <typename T> struct Planes {
     const T *wo_m, *wo_0, *wo_p;  // previous z faces, face-planes k-1, k, k+1
 };
 
+// Every staged value the three high faces of one cell read.  Names: plane
+// prefix (none = plane k, P = k+1, M = k-1 for c; u/v/w = previous faces,
+// p = plane k+1, m = face-plane k-1) then the offset (L/R = x -+ 1, D/U =
+// y -+ 1, L2 = x - 2).
+template <typename T> struct Nb {
+    T C, L, R, D, Uu, RU, RD, LU;   // c, plane k
+    T P, PL, PR, PD, PU;            // c, plane k+1
+    T M, MR, MU;                    // c, plane k-1
+    T u, uL, uR, uL2, uLU, uU, uL2U;  // x faces, plane k
+    T up, upL;                      // x faces, plane k+1
+    T v, vD, vU, vR, vRD;           // y faces, plane k
+    T vp, vpD;                      // y faces, plane k+1
+    T wm, wmR, wmU;                 // z faces, face-plane k-1
+    T w, wR, wU;                    // z faces, face-plane k
+    T wp;                           // z faces, face-plane k+1
+};
+
+template <typename T>
+__device__ __forceinline__ Nb<T> gather(const Planes<T>& S, int o, T own_m, T own_p)
+{
+    constexpr int Y = SBX;
+    Nb<T> n;
+    n.C = S.c_0[o]; n.L = S.c_0[o - 1]; n.R = S.c_0[o + 1]; n.D = S.c_0[o - Y];
+    n.Uu = S.c_0[o + Y]; n.RU = S.c_0[o + 1 + Y]; n.RD = S.c_0[o + 1 - Y]; n.LU = S.c_0[o - 1 + Y];
+    n.P = own_p; n.PL = S.c_p[o - 1]; n.PR = S.c_p[o + 1]; n.PD = S.c_p[o - Y]; n.PU = S.c_p[o + Y];
+    n.M = own_m; n.MR = S.c_m[o + 1]; n.MU = S.c_m[o + Y];
+    n.u = S.uo_0[o]; n.uL = S.uo_0[o - 1]; n.uR = S.uo_0[o + 1]; n.uL2 = S.uo_0[o - 2];
+    n.uLU = S.uo_0[o - 1 + Y]; n.uU = S.uo_0[o + Y]; n.uL2U = S.uo_0[o - 2 + Y];
+    n.up = S.uo_p[o]; n.upL = S.uo_p[o - 1];
+    n.v = S.vo_0[o]; n.vD = S.vo_0[o - Y]; n.vU = S.vo_0[o + Y]; n.vR = S.vo_0[o + 1];
+    n.vRD = S.vo_0[o + 1 - Y];
+    n.vp = S.vo_p[o]; n.vpD = S.vo_p[o - Y];
+    n.wm = S.wo_m[o]; n.wmR = S.wo_m[o + 1]; n.wmU = S.wo_m[o + Y];
+    n.w = S.wo_0[o]; n.wR = S.wo_0[o + 1]; n.wU = S.wo_0[o + Y];
+    n.wp = S.wo_p[o];
+    return n;
+}
+
 struct FaceCtx {
     int nx, ny, ns, use_div, vv_fix, pass;
 };
 
-// x face between cells i and i+1 (row j, plane k); o = staged offset of cell i.
-template <typename T>
-__device__ __forceinline__ T face_u(const Planes<T>& P, int o, int i, const FaceCtx& f)
+template <int V> struct IC {
+    static constexpr int value = V;
+};
+
+// x face between cells i and i+1.
+template <bool AP, typename T> __device__ __forceinline__ T face_u(const Nb<T>& n, int i, const FaceCtx& f)
 {
-    constexpr int Y = SBX;
     T vb, wb, neg_div = T(0);
-    if (i == 0 || i == f.nx - 2) {
-        const int a = (i == 0) ? o + 1 : o;
-        vb = T(0.5) * (P.vo_0[a - Y] + P.vo_0[a]);
-        wb = T(0.5) * (P.wo_m[a] + P.wo_0[a]);
+    if (i == 0) {
+        vb = T(0.5) * (n.vRD + n.vR);
+        wb = T(0.5) * (n.wmR + n.wR);
+    } else if (i == f.nx - 2) {
+        vb = T(0.5) * (n.vD + n.v);
+        wb = T(0.5) * (n.wm + n.w);
     } else {
-        vb = T(0.25) * (((P.vo_0[o + 1 - Y] + P.vo_0[o + 1]) + P.vo_0[o]) + P.vo_0[o - Y]);
-        wb = T(0.25) * (((P.wo_m[o + 1] + P.wo_0[o + 1]) + P.wo_0[o]) + P.wo_m[o]);
+        vb = T(0.25) * (((n.vRD + n.vR) + n.v) + n.vD);
+        wb = T(0.25) * (((n.wmR + n.wR) + n.w) + n.wm);
         if (f.use_div) {
-            T s = P.uo_0[o + 1] - P.uo_0[o - 1];
-            s = s + P.vo_0[o + 1 - Y];
-            s = s - P.vo_0[o + 1];
-            s = s - P.vo_0[o];
-            s = s + P.vo_0[o - Y];
-            s = s + P.wo_m[o + 1];
-            s = s - P.wo_0[o + 1];
-            s = s - P.wo_0[o];
-            s = s + P.wo_m[o];
-            neg_div = -((T(0.25) * P.uo_0[o]) * s);
+            T s = n.uR - n.uL;
+            s = s + n.vRD;
+            s = s - n.vR;
+            s = s - n.v;
+            s = s + n.vD;
+            s = s + n.wmR;
+            s = s - n.wR;
+            s = s - n.w;
+            s = s + n.wm;
+            neg_div = -((T(0.25) * n.u) * s);
         } else {
             neg_div = -T(0);
         }
     }
     T n1, d1, n2, d2;
-    grad_pair(P.c_0[o + 1 + Y], P.c_0[o + Y], P.c_0[o - Y], P.c_0[o + 1 - Y], n1, d1);
-    grad_pair(P.c_p[o + 1], P.c_p[o], P.c_m[o], P.c_m[o + 1], n2, d2);
-    return face_pattern(neg_div, P.uo_0[o], P.c_0[o], P.c_0[o + 1], vb, n1, d1, wb, n2, d2);
+    grad_pair(n.RU, n.Uu, n.D, n.RD, n1, d1);
+    grad_pair(n.PR, n.P, n.M, n.MR, n2, d2);
+    return face_pattern<T, AP>(neg_div, n.u, n.C, n.R, vb, n1, d1, wb, n2, d2);
 }
 
 // y face between rows j and j+1 (column i, plane k).
-template <typename T>
-__device__ __forceinline__ T face_v(const Planes<T>& P, int o, int i, int j, int k,
-                                   const FaceCtx& f, const Dims& d, const T* __restrict__ Vadv)
+template <bool AP, typename T>
+__device__ __forceinline__ T face_v(const Nb<T>& n, int i, int j, int k, const FaceCtx& f,
+                                   const Dims& d, const T* __restrict__ Vadv)
 {
-    constexpr int Y = SBX;
     T ub, wb, neg_div = T(0);
-    if (j == 0 || j == f.ny - 2) {
-        const int a = (j == 0) ? o + Y : o;
-        ub = T(0.5) * (P.uo_0[a - 1] + P.uo_0[a]);
-        wb = T(0.5) * (P.wo_m[a] + P.wo_0[a]);
+    if (j == 0) {
+        ub = T(0.5) * (n.uLU + n.uU);
+        wb = T(0.5) * (n.wmU + n.wU);
+    } else if (j == f.ny - 2) {
+        ub = T(0.5) * (n.uL + n.u);
+        wb = T(0.5) * (n.wm + n.w);
     } else {
         if (i == 1 && !f.vv_fix)  // the column vv_pass never writes (vv.c:81-82)
             return (f.pass & 1) ? T(0) : Vadv[cell(d, 1, j, k)];
-        ub = T(0.25) * (((P.uo_0[o - 1 + Y] + P.uo_0[o + Y]) + P.uo_0[o]) + P.uo_0[o - 1]);
-        wb = T(0.25) * (((P.wo_m[o + Y] + P.wo_0[o + Y]) + P.wo_0[o]) + P.wo_m[o]);
+        ub = T(0.25) * (((n.uLU + n.uU) + n.u) + n.uL);
+        wb = T(0.25) * (((n.wmU + n.wU) + n.w) + n.wm);
         if (f.use_div) {
-            const T ul2u = (i >= 2) ? P.uo_0[o - 2 + Y] : T(0);
-            const T ul2 = (i >= 2) ? P.uo_0[o - 2] : T(0);
-            T s = P.vo_0[o + Y] - P.vo_0[o - Y];
-            s = s + P.wo_m[o + Y];
-            s = s - P.wo_0[o + Y];
-            s = s - P.wo_0[o];
-            s = s + P.wo_m[o];
-            s = s + P.uo_0[o - 1 + Y];
+            const T ul2u = (i >= 2) ? n.uL2U : T(0);
+            const T ul2 = (i >= 2) ? n.uL2 : T(0);
+            T s = n.vU - n.vD;
+            s = s + n.wmU;
+            s = s - n.wU;
+            s = s - n.w;
+            s = s + n.wm;
+            s = s + n.uLU;
             s = s - ul2u;
             s = s - ul2;
-            s = s + P.uo_0[o - 1];
-            neg_div = -((T(0.25) * P.vo_0[o]) * s);
+            s = s + n.uL;
+            neg_div = -((T(0.25) * n.v) * s);
         } else {
             neg_div = -T(0);
         }
     }
     T n1, d1, n2, d2;
-    grad_pair(P.c_0[o + 1 + Y], P.c_0[o + 1], P.c_0[o - 1], P.c_0[o - 1 + Y], n1, d1);
-    grad_pair(P.c_p[o + Y], P.c_p[o], P.c_m[o], P.c_m[o + Y], n2, d2);
-    return face_pattern(neg_div, P.vo_0[o], P.c_0[o], P.c_0[o + Y], ub, n1, d1, wb, n2, d2);
+    grad_pair(n.RU, n.R, n.L, n.LU, n1, d1);
+    grad_pair(n.PU, n.P, n.M, n.MU, n2, d2);
+    return face_pattern<T, AP>(neg_div, n.v, n.C, n.Uu, ub, n1, d1, wb, n2, d2);
 }
 
-// z face between planes k and k+1 (cell column i, j).
-template <typename T>
-__device__ __forceinline__ T face_w(const Planes<T>& P, int o, int k, const FaceCtx& f)
+// z face between planes k and k+1.
+template <bool AP, typename T> __device__ __forceinline__ T face_w(const Nb<T>& n, int k, const FaceCtx& f)
 {
-    constexpr int Y = SBX;
     T ub, vb, neg_div = T(0);
-    if (k == 0 || k == f.ns - 2) {
-        const T* U = (k == 0) ? P.uo_p : P.uo_0;  // the interior plane next to the face
-        const T* V = (k == 0) ? P.vo_p : P.vo_0;
-        ub = T(0.5) * (U[o - 1] + U[o]);
-        vb = T(0.5) * (V[o - Y] + V[o]);
+    if (k == 0) {
+        ub = T(0.5) * (n.upL + n.up);
+        vb = T(0.5) * (n.vpD + n.vp);
+    } else if (k == f.ns - 2) {
+        ub = T(0.5) * (n.uL + n.u);
+        vb = T(0.5) * (n.vD + n.v);
     } else {
-        ub = T(0.25) * (((P.uo_0[o] + P.uo_p[o]) + P.uo_p[o - 1]) + P.uo_0[o - 1]);
-        vb = T(0.25) * (((P.vo_p[o - Y] + P.vo_p[o]) + P.vo_0[o]) + P.vo_0[o - Y]);
+        ub = T(0.25) * (((n.u + n.up) + n.upL) + n.uL);
+        vb = T(0.25) * (((n.vpD + n.vp) + n.v) + n.vD);
         if (f.use_div) {
-            T s = P.wo_p[o] - P.wo_m[o];
-            s = s + P.uo_p[o - 1];
-            s = s - P.uo_p[o];
-            s = s - P.uo_0[o];
-            s = s + P.uo_0[o - 1];
-            s = s + P.vo_p[o - Y];
-            s = s - P.vo_p[o];
-            s = s - P.vo_0[o];
-            s = s + P.vo_0[o - Y];
-            neg_div = -((T(0.25) * P.wo_0[o]) * s);
+            T s = n.wp - n.wm;
+            s = s + n.upL;
+            s = s - n.up;
+            s = s - n.u;
+            s = s + n.uL;
+            s = s + n.vpD;
+            s = s - n.vp;
+            s = s - n.v;
+            s = s + n.vD;
+            neg_div = -((T(0.25) * n.w) * s);
         } else {
             neg_div = -T(0);
         }
     }
     T n1, d1, n2, d2;
-    grad_pair(P.c_p[o + 1], P.c_0[o + 1], P.c_0[o - 1], P.c_p[o - 1], n1, d1);
-    grad_pair(P.c_p[o + Y], P.c_0[o + Y], P.c_0[o - Y], P.c_p[o - Y], n2, d2);
-    return face_pattern(neg_div, P.wo_0[o], P.c_0[o], P.c_p[o], ub, n1, d1, vb, n2, d2);
+    grad_pair(n.PR, n.R, n.L, n.PL, n1, d1);
+    grad_pair(n.PU, n.Uu, n.D, n.PD, n2, d2);
+    return face_pattern<T, AP>(neg_div, n.w, n.C, n.P, ub, n1, d1, vb, n2, d2);
 }
 
 }  // namespace fused
 
-template <typename T, bool LIM, typename A>
+template <typename T, bool LIM, typename A, bool AP>
 __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
     k_pass_tma(Dims d, PassArgs<T> a, const __grid_constant__ CUtensorMap map_c,
                const __grid_constant__ CUtensorMap map_cn, const __grid_constant__ CUtensorMap map_uo,
@@ -209,6 +254,17 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
     const FaceCtx fc{nx, ny, ns, a.use_div, a.vv_fix, a.pass};
     const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
     const bool owned = cell_in && (!LIM || (x >= 1 && x <= BX - 2 && y >= 1 && y <= BY - 2));
+    const bool u_ok = i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2;  // own x face exists
+    const bool v_ok = i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2;  // own y face exists
+    // Extra faces below the column: threads 0..BY-1 the x faces at local x = -1,
+    // threads BY..BY+BX-1 the y faces at local y = -1.
+    const bool ex_u = tid < BY, ex_v = tid >= BY && tid < BY + BX;
+    const int ex_i = ex_u ? i0 - 1 : i0 + (tid - BY);
+    const int ex_j = ex_u ? j0 + tid : j0 - 1;
+    const int ex_o = ex_u ? (tid + 2) * Y + (1 + rx) : Y + (tid - BY + 2 + rx);
+    const int ex_w = ex_u ? (tid + 1) * WX : (tid - BY + 1);
+    const bool ex_ok = ex_u ? (ex_i >= 0 && ex_i <= nx - 2 && ex_j >= 1 && ex_j <= ny - 2)
+                            : (ex_v && ex_i >= 1 && ex_i <= nx - 2 && ex_j >= 0 && ex_j <= ny - 2);
 
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) tma::mbar_init(&bars[s], 1);
@@ -225,20 +281,16 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
         uint64_t* bar = &bars[p & (NSTAGE - 1)];
         tma::fence_proxy_async_shared();
         tma::mbar_arrive_expect_tx(bar, (uint32_t)(NARR * SBX * SBY * sizeof(T)));
-        T* dst = const_cast<T*>(box(p, 0));
-        tma::load_3d(dst, &map_c, gx0, gy0, p, bar);
+        tma::load_3d(const_cast<T*>(box(p, 0)), &map_c, gx0, gy0, p, bar);
         tma::load_3d(const_cast<T*>(box(p, 1)), &map_uo, gx0, gy0, p, bar);
         tma::load_3d(const_cast<T*>(box(p, 2)), &map_vo, gx0, gy0, p, bar);
         tma::load_3d(const_cast<T*>(box(p, 3)), &map_wo, gx0, gy0, p, bar);
         if (LIM) tma::load_3d(const_cast<T*>(box(p, 4)), &map_cn, gx0, gy0, p, bar);
     };
-    auto planes = [&](int k) {
-        Planes<T> P;
-        P.c_m = box(k - 1, 0); P.c_0 = box(k, 0); P.c_p = box(k + 1, 0);
-        P.uo_0 = box(k, 1); P.uo_p = box(k + 1, 1);
-        P.vo_0 = box(k, 2); P.vo_p = box(k + 1, 2);
-        P.wo_m = box(k - 1, 3); P.wo_0 = box(k, 3); P.wo_p = box(k + 1, 3);
-        return P;
+    // Stage slot s of array arr (s is a compile-time constant at every use:
+    // the march below is unrolled by the ring depth).
+    auto slot = [&](int s, int arr) -> const T* {
+        return reinterpret_cast<const T*>(smem + (size_t)(s * NARR + arr) * SB);
     };
 
     bool ok = true;
@@ -257,38 +309,44 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
     T lu_prev = T(0), lv_prev = T(0), lw_prev = T(0);  // limited faces of plane k-1 / face-plane k-2
 
     const int last = LIM ? ns - 1 : ns - 2;
-    for (int k = 0; k <= last; k++) {
+    // One plane of the march; S = k mod NSTAGE (compile-time).
+    auto plane = [&](auto Sc, const int k) {
+        constexpr int S = decltype(Sc)::value;
+        constexpr int SM1 = (S + NSTAGE - 1) % NSTAGE, SP1 = (S + 1) % NSTAGE, SP2 = (S + 2) % NSTAGE;
         __syncthreads();  // every read of the slot plane k+2 reuses is done
         if (tid == 0 && k + 2 <= ns - 1) issue(k + 2);
         if (k + 1 <= ns - 1) {
-            if (ok) ok = tma::mbar_wait(&bars[(k + 1) & (NSTAGE - 1)], ((k + 1) / NSTAGE) & 1);
+            if (ok) ok = tma::mbar_wait(&bars[SP1], ((k + 1) / NSTAGE) & 1);
             if (tid == 0 && ok) confirmed = k + 2;
-            cq3 = box(k + 1, 0)[o];
+            cq3 = slot(SP1, 0)[o];
         }
+        (void)SP2;
         const bool kin = k >= 1 && k <= ns - 2;
 
         // ---- raw faces of plane k (z face: face-plane k) ----
         T ru = T(0), rv = T(0), rw = T(0);
         if (k <= ns - 2) {
-            const Planes<T> P = planes(k);
-            if (kin && i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2) ru = face_u(P, o, i, fc);
-            if (kin && i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2)
-                rv = face_v(P, o, i, j, k, fc, d, a.Vadv);
-            if (cell_in) rw = face_w(P, o, k, fc);
+            Planes<T> SP;
+            SP.c_m = slot(SM1, 0); SP.c_0 = slot(S, 0); SP.c_p = slot(SP1, 0);
+            SP.uo_0 = slot(S, 1); SP.uo_p = slot(SP1, 1);
+            SP.vo_0 = slot(S, 2); SP.vo_p = slot(SP1, 2);
+            SP.wo_m = slot(SM1, 3); SP.wo_0 = slot(S, 3); SP.wo_p = slot(SP1, 3);
+            {
+                const Nb<T> nb = gather(SP, o, cq1, cq3);
+                if (kin && u_ok) ru = face_u<AP>(nb, i, fc);
+                if (kin && v_ok) rv = face_v<AP>(nb, i, j, k, fc, d, a.Vadv);
+                if (cell_in) rw = face_w<AP>(nb, k, fc);
+            }
             sRU[w] = ru;
             sRV[w] = rv;
-            if (tid < BY) {  // x faces just left of the column
-                const int ye = tid, ie = i0 - 1, je = j0 + ye;
-                T v = T(0);
-                if (kin && ie >= 0 && ie <= nx - 2 && je >= 1 && je <= ny - 2)
-                    v = face_u(P, (ye + 2) * Y + (1 + rx), ie, fc);
-                sRU[(ye + 1) * WX] = v;
-            } else if (tid < BY + BX) {  // y faces just below the column
-                const int xe = tid - BY, ie = i0 + xe, je = j0 - 1;
-                T v = T(0);
-                if (kin && ie >= 1 && ie <= nx - 2 && je >= 0 && je <= ny - 2)
-                    v = face_v(P, Y + (xe + 2 + rx), ie, je, k, fc, d, a.Vadv);
-                sRV[xe + 1] = v;
+            if (ex_u || ex_v) {
+                T ev = T(0);
+                if (kin && ex_ok) {
+                    const Nb<T> nb = gather(SP, ex_o, SP.c_m[ex_o], SP.c_p[ex_o]);
+                    ev = ex_u ? face_u<AP>(nb, ex_i, fc)
+                              : face_v<AP>(nb, ex_i, ex_j, k, fc, d, a.Vadv);
+                }
+                (ex_u ? sRU : sRV)[ex_w] = ev;
             }
         }
         __syncthreads();
@@ -297,30 +355,29 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
             // ---- limiter ratios of plane k ----
             T bu = T(1), bd = T(1);
             if (kin && cell_in) {
-                const T* c0 = box(k, 0);
-                const T* n0 = box(k, 4);
+                const T* c0 = slot(S, 0);
+                const T* n0 = slot(S, 4);
                 const T psi = cq2;
-                T mx = psi, mn = psi, t;
-#define MPD_BOUND(v) do { t = (v); mx = t > mx ? t : mx; mn = t < mn ? t : mn; } while (0)
-                MPD_BOUND(n0[o]);
-                MPD_BOUND(c0[o - 1]); MPD_BOUND(n0[o - 1]);
-                MPD_BOUND(c0[o + 1]); MPD_BOUND(n0[o + 1]);
-                MPD_BOUND(c0[o - Y]); MPD_BOUND(n0[o - Y]);
-                MPD_BOUND(c0[o + Y]); MPD_BOUND(n0[o + Y]);
+                const T cl = c0[o - 1], cr = c0[o + 1], cd = c0[o - Y], cu = c0[o + Y];
+                T mx = vmax(psi, n0[o]), mn = vmin(psi, n0[o]);
+                mx = vmax(vmax(cl, n0[o - 1]), mx); mn = vmin(vmin(cl, n0[o - 1]), mn);
+                mx = vmax(vmax(cr, n0[o + 1]), mx); mn = vmin(vmin(cr, n0[o + 1]), mn);
+                mx = vmax(vmax(cd, n0[o - Y]), mx); mn = vmin(vmin(cd, n0[o - Y]), mn);
+                mx = vmax(vmax(cu, n0[o + Y]), mx); mn = vmin(vmin(cu, n0[o + Y]), mn);
                 if (ns > 3) {
-                    MPD_BOUND(cq1); MPD_BOUND(box(k - 1, 4)[o]);
-                    MPD_BOUND(cq3); MPD_BOUND(box(k + 1, 4)[o]);
+                    const T nm = slot(SM1, 4)[o], np = slot(SP1, 4)[o];
+                    mx = vmax(vmax(cq1, nm), mx); mn = vmin(vmin(cq1, nm), mn);
+                    mx = vmax(vmax(cq3, np), mx); mn = vmin(vmin(cq3, np), mn);
                 }
-#undef MPD_BOUND
                 A fin = A(0), fout = A(0);
-                lim_acc(lim_flux<T, A>(sRU[w - 1], c0[o - 1], psi), false, fin, fout);
-                lim_acc(lim_flux<T, A>(ru, psi, c0[o + 1]), true, fin, fout);
-                lim_acc(lim_flux<T, A>(sRV[w - WX], c0[o - Y], psi), false, fin, fout);
-                lim_acc(lim_flux<T, A>(rv, psi, c0[o + Y]), true, fin, fout);
+                lim_acc(lim_flux<T, A>(sRU[w - 1], cl, psi), false, fin, fout);
+                lim_acc(lim_flux<T, A>(ru, psi, cr), true, fin, fout);
+                lim_acc(lim_flux<T, A>(sRV[w - WX], cd, psi), false, fin, fout);
+                lim_acc(lim_flux<T, A>(rv, psi, cu), true, fin, fout);
                 lim_acc(lim_flux<T, A>(rw_prev, cq1, psi), false, fin, fout);
                 lim_acc(lim_flux<T, A>(rw, psi, cq3), true, fin, fout);
-                bu = T((A(mx) - A(psi)) / (fin + lim_tiny<A>()));
-                bd = T((A(psi) - A(mn)) / (fout + lim_tiny<A>()));
+                bu = T(ratio<AP>(A(mx) - A(psi), fin + lim_tiny<A>()));
+                bd = T(ratio<AP>(A(psi) - A(mn), fout + lim_tiny<A>()));
             }
             sBU[w] = bu;
             sBD[w] = bd;
@@ -331,24 +388,22 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
             if (x < BX - 1) lu = limit_face(ru, bu, bd, sBU[w + 1], sBD[w + 1]);
             if (y < BY - 1) lv = limit_face(rv, bu, bd, sBU[w + WX], sBD[w + WX]);
             const T lw = limit_face(rw_prev, bu_prev, bd_prev, bu, bd);
-            sLU[(k & 1) * WPL + w] = lu;
-            sLV[(k & 1) * WPL + w] = lv;
+            sLU[(S & 1) * WPL + w] = lu;
+            sLV[(S & 1) * WPL + w] = lv;
             if (a.write_faces) {
                 const bool ox = x >= 1 && x <= BX - 2, oy = y >= 1 && y <= BY - 2;
                 const long long q = cell(d, i, j, k);
-                if (kin && i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2 && oy && (ox || i == 0))
-                    a.Un[q] = lu;
-                if (kin && i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2 && ox && (oy || j == 0))
-                    a.Vn[q] = lv;
+                if (kin && u_ok && oy && (ox || i == 0)) a.Un[q] = lu;
+                if (kin && v_ok && ox && (oy || j == 0)) a.Vn[q] = lv;
                 if (k >= 1 && owned) a.Wn[q - d.pp] = lw;
             }
 
             // ---- donor update of plane k-1 ----
             const int u = k - 1;
             if (u >= 1 && u <= ns - 2 && owned) {
-                const T* cu = box(u, 0);
-                const T ul = sLU[(u & 1) * WPL + w - 1];
-                const T vb = sLV[(u & 1) * WPL + w - WX];
+                const T* cu = slot(SM1, 0);
+                const T ul = sLU[(SM1 & 1) * WPL + w - 1];
+                const T vb = sLV[(SM1 & 1) * WPL + w - WX];
                 a.c_out[cell(d, i, j, u)] =
                     donor_update(cu[o], cu[o - 1], cu[o + 1], cu[o - Y], cu[o + Y], cq0, cq2, lu_prev,
                                  ul, lv_prev, vb, lw, lw_prev);
@@ -361,7 +416,7 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
         } else {
             // ---- donor update of plane k ----
             if (kin && owned) {
-                const T* c0 = box(k, 0);
+                const T* c0 = slot(S, 0);
                 const T ul = sRU[w - 1], vb = sRV[w - WX];
                 const long long q = cell(d, i, j, k);
                 a.c_out[q] = donor_update(c0[o], c0[o - 1], c0[o + 1], c0[o - Y], c0[o + Y], cq1,
@@ -380,6 +435,12 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
         cq0 = cq1;
         cq1 = cq2;
         cq2 = cq3;
+    };
+    for (int kb = 0; kb <= last; kb += NSTAGE) {
+        plane(IC<0>{}, kb);
+        if (kb + 1 <= last) plane(IC<1>{}, kb + 1);
+        if (kb + 2 <= last) plane(IC<2>{}, kb + 2);
+        if (kb + 3 <= last) plane(IC<3>{}, kb + 3);
     }
 
     if (!ok && a.err) atomicOr(a.err, 1);
@@ -389,14 +450,14 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
     }
 }
 
-template <typename T, bool LIM, typename A>
+template <typename T, bool LIM, typename A, bool AP>
 int launch_fused_variant(const Dims& d, const PassArgs<T>& a, cudaStream_t s)
 {
     using namespace fused;
     constexpr size_t smem = smem_bytes<T, LIM>();
     static bool configured = false;  // the attribute is per device function
     if (!configured) {
-        cudaFuncSetAttribute(k_pass_tma<T, LIM, A>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_pass_tma<T, LIM, A, AP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         configured = true;
     }
@@ -404,15 +465,21 @@ int launch_fused_variant(const Dims& d, const PassArgs<T>& a, cudaStream_t s)
     dim3 g((d.nx - 2 + BX - 2 * OW - 1) / (BX - 2 * OW), (d.ny - 2 + BY - 2 * OW - 1) / (BY - 2 * OW));
     dim3 b(BX, BY);
     const CUtensorMap& cn = LIM ? *a.maps.cn : *a.maps.c;
-    k_pass_tma<T, LIM, A><<<g, b, smem, s>>>(d, a, *a.maps.c, cn, *a.maps.uo, *a.maps.vo,
-                                             *a.maps.wo);
+    k_pass_tma<T, LIM, A, AP><<<g, b, smem, s>>>(d, a, *a.maps.c, cn, *a.maps.uo, *a.maps.vo,
+                                                 *a.maps.wo);
     return 1;
+}
+
+template <typename T, bool AP> int launch_fused_mode(const Dims& d, const PassArgs<T>& a, cudaStream_t s)
+{
+    if (!a.limiter) return launch_fused_variant<T, false, T, AP>(d, a, s);
+    if (a.wide) return launch_fused_variant<T, true, double, AP>(d, a, s);
+    return launch_fused_variant<T, true, T, AP>(d, a, s);
 }
 
 template <typename T>
 int launch_pass_fused(const Dims& d, const PassArgs<T>& a, cudaStream_t s)
 {
-    if (!a.limiter) return launch_fused_variant<T, false, T>(d, a, s);
-    if (a.wide) return launch_fused_variant<T, true, double>(d, a, s);
-    return launch_fused_variant<T, true, T>(d, a, s);
+    if (a.approx && sizeof(T) == 4) return launch_fused_mode<T, true>(d, a, s);
+    return launch_fused_mode<T, false>(d, a, s);
 }

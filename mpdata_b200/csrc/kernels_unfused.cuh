@@ -177,7 +177,7 @@ __global__ void k_fct_beta(Dims d, const T* __restrict__ c, const T* __restrict_
     const long long q = cell(d, i, j, k);
     T psi = c[q];
     T mx = psi, mn = psi, t;
-#define MPD_BOUND(v) do { t = (v); mx = t > mx ? t : mx; mn = t < mn ? t : mn; } while (0)
+#define MPD_BOUND(v) do { t = (v); mx = vmax(t, mx); mn = vmin(t, mn); } while (0)
     MPD_BOUND(cn[q]);
     MPD_BOUND(c[q - X]); MPD_BOUND(cn[q - X]);
     MPD_BOUND(c[q + X]); MPD_BOUND(cn[q + X]);

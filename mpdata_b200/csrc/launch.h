@@ -46,6 +46,7 @@ template <typename T> struct PassArgs {
     int limiter;       // FCT on
     int wide;          // FP64 limiter ratios (float storage only)
     int write_faces;   // the next pass reads Un/Vn/Wn
+    int approx;        // fused FP32 path: hardware-reciprocal ratios (approx_div form)
 };
 
 #define MPD_DECLARE_LAUNCHERS                                                              \

@@ -302,6 +302,7 @@ template <typename T> int step_impl(Solver* h, int nsteps)
             a.limiter = h->opts.limiter;
             a.wide = h->opts.precision_form;
             a.write_faces = o < P - 1;
+            a.approx = h->opts.approx_div;
             {
                 PassTimer timer(h, a.write_faces ? 1 : 2);
                 if (fused) op.pass_fused(d, a, h->stream);
@@ -428,6 +429,8 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     if (o.precision_form && dtype != MPDATA_F32)
         return fail(MPDATA_ERR_ARG, "precision_form applies to float storage only");
     if (o.kernel < 0 || o.kernel > 1) return fail(MPDATA_ERR_ARG, "bad kernel option %d", o.kernel);
+    if (o.approx_div && (dtype != MPDATA_F32 || o.strict || o.kernel != 0))
+        return fail(MPDATA_ERR_ARG, "approx_div needs float storage, fused kernels and no strict mode");
     std::unique_ptr<Solver> h(new Solver());
     h->dtype = dtype;
     h->esz = dtype == MPDATA_F32 ? 4 : 8;

@@ -294,7 +294,7 @@ static void SFX(fct_limit)(int nx, int ny, int ns, const R* c, const R* cn, R* U
             for (int i = 1; i < nx - 1; i++) {
                 R psi = AT(c, i, j, k);
                 R mx = psi, mn = psi, t;
-#define BOUND(a) do { t = (a); mx = t > mx ? t : mx; mn = t < mn ? t : mn; } while (0)
+#define BOUND(a) do { t = (a); mx = RMAX(t, mx); mn = RMIN(t, mn); } while (0)
                 BOUND(AT(cn, i, j, k));
                 BOUND(AT(c, i - 1, j, k)); BOUND(AT(cn, i - 1, j, k));
                 BOUND(AT(c, i + 1, j, k)); BOUND(AT(cn, i + 1, j, k));

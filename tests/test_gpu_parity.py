@@ -139,6 +139,29 @@ def test_handle_default_mode_within_tolerance(m, dtype, limiter):
     assert np.abs(got - ref).max() <= TOL[np.dtype(dtype)]
 
 
+@pytest.mark.parametrize("limiter", [0, 1])
+@pytest.mark.parametrize("precision_form", [0, 1])
+def test_approx_div_within_tolerance(m, limiter, precision_form):
+    """Hardware-reciprocal ratios (approx_div): FP32 max-abs <= 1e-5 against
+    the IEEE oracle after 5 steps of IORD 3."""
+    import oracle
+    if precision_form and not limiter:
+        pytest.skip("the precision form only changes the limiter")
+    case = workloads.random_case(66, 30, 12, seed=12)
+    U, V, W = _faces(case, np.float32)
+    c = case["c0"].astype(np.float32)
+    ref = c
+    for _ in range(5):
+        ref = oracle.step_faces(U, V, W, ref, 3, limiter=limiter, wide_beta=precision_form)
+    with m.Solver(66, 30, 12, order=3, limiter=bool(limiter), approx_div=True,
+                  precision_form=bool(precision_form)) as s:
+        s.set_faces(U, V, W)
+        s.set_field(c)
+        s.step(5)
+        got = s.get_field()
+    assert np.abs(got - ref).max() <= TOL[np.dtype(np.float32)]
+
+
 def test_previous_level_matches_oracle(m):
     import oracle
     case = workloads.random_case(37, 11, 6, seed=2)
