@@ -192,6 +192,39 @@ int mpdata_launches_per_step(mpdata_handle h);
 int mpdata_enable_pass_timing(mpdata_handle h, int on);
 int mpdata_pass_times(mpdata_handle h, double ms[3], long long launches[3], int reset);
 
+/* ---- Batched ensemble of independent 2D problems --------------------------
+ *
+ * No reference counterpart (the reference steps one grid per smolar() call).
+ * n instances of uneven size nx[q] x ny[q] (each the 2D form: the reference's
+ * nx x ny x 3 grid with w = 0, fixed one-cell shell), float storage, one
+ * common order and option set.  Every pass covers all instances in one
+ * launch; mpdata_ensemble_step replays a CUDA graph of nsteps steps (captured
+ * on first use per step count).  2D arrays are ny x nx, x fastest; U is the
+ * face between cells i and i+1, V between rows j and j+1 (as in
+ * mpdata_set_faces). */
+typedef struct mpdata_ensemble* mpdata_ensemble_handle;
+
+int mpdata_ensemble_create(mpdata_ensemble_handle* e, int n, const int* nx, const int* ny,
+                           int order, const struct mpdata_options* opts);
+int mpdata_ensemble_destroy(mpdata_ensemble_handle e);
+int mpdata_ensemble_set_stream(mpdata_ensemble_handle e, void* stream);
+int mpdata_ensemble_set_faces(mpdata_ensemble_handle e, int q, const void* U, const void* V,
+                              int where);
+int mpdata_ensemble_set_field(mpdata_ensemble_handle e, int q, const void* c, int where);
+int mpdata_ensemble_get_field(mpdata_ensemble_handle e, int q, void* c, int where);
+/* nsteps steps of every instance, as one CUDA graph launch (asynchronous). */
+int mpdata_ensemble_step(mpdata_ensemble_handle e, int nsteps);
+/* The same steps as individual kernel launches (no graph). */
+int mpdata_ensemble_step_direct(mpdata_ensemble_handle e, int nsteps);
+int mpdata_ensemble_sync(mpdata_ensemble_handle e);
+/* Time every tile-shape candidate over trial_steps steps on the ensemble
+ * itself and keep the fastest (*chosen = its index, *ms_per_step = its time).
+ * The trials advance the instances: set the fields again afterwards. */
+int mpdata_ensemble_autotune(mpdata_ensemble_handle e, int trial_steps, int* chosen,
+                             double* ms_per_step);
+/* Force a tile-shape candidate (0: 32x8, 1: 32x16, 2: 64x8 threads). */
+int mpdata_ensemble_tile(mpdata_ensemble_handle e, int tile);
+
 /* ---- 3. Allocation-free step --------------------------------------------
  *
  * No counterpart in the reference.  One FP32 step (`order` passes, optional

@@ -78,6 +78,18 @@ _lib.mpdata_host_alloc.argtypes = [C.c_size_t]
 _lib.mpdata_host_free.argtypes = [_vp]
 _lib.msmolar_free.argtypes = [C.POINTER(_vp)]
 _lib.mpdata_set_default_options.argtypes = [C.POINTER(Options)]
+_lib.mpdata_ensemble_create.argtypes = [C.POINTER(_vp), C.c_int, C.POINTER(C.c_int),
+                                        C.POINTER(C.c_int), C.c_int, C.POINTER(Options)]
+_lib.mpdata_ensemble_destroy.argtypes = [_vp]
+_lib.mpdata_ensemble_set_stream.argtypes = [_vp, _vp]
+_lib.mpdata_ensemble_set_faces.argtypes = [_vp, C.c_int, _vp, _vp, C.c_int]
+_lib.mpdata_ensemble_set_field.argtypes = [_vp, C.c_int, _vp, C.c_int]
+_lib.mpdata_ensemble_get_field.argtypes = [_vp, C.c_int, _vp, C.c_int]
+_lib.mpdata_ensemble_step.argtypes = [_vp, C.c_int]
+_lib.mpdata_ensemble_step_direct.argtypes = [_vp, C.c_int]
+_lib.mpdata_ensemble_sync.argtypes = [_vp]
+_lib.mpdata_ensemble_autotune.argtypes = [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+_lib.mpdata_ensemble_tile.argtypes = [_vp, C.c_int]
 _lib.mpdata_enable_pass_timing.argtypes = [_vp, C.c_int]
 _lib.mpdata_pass_times.argtypes = [_vp, C.POINTER(C.c_double * 3), C.POINTER(C.c_longlong * 3),
                                    C.c_int]
@@ -329,3 +341,78 @@ class Solver:
         n = (C.c_longlong * 3)()
         _check(_lib.mpdata_pass_times(self._h, C.byref(ms), C.byref(n), int(reset)))
         return list(ms), list(n)
+
+
+class Ensemble:
+    """Batched ensemble of independent 2D problems (``mpdata_ensemble_*``).
+
+    Instance q is an ``ny[q] x nx[q]`` grid (the reference's 2D form:
+    ``nx x ny x 3`` with w = 0), float32.  Faces and fields are 2D arrays of
+    shape ``(ny, nx)``."""
+
+    TILES = ((32, 8), (32, 16), (64, 8))
+
+    def __init__(self, nx, ny, order: int = 2, options: SolverOptions | None = None, **kw):
+        opts = options or SolverOptions(**kw)
+        self.nx = [int(v) for v in nx]
+        self.ny = [int(v) for v in ny]
+        if len(self.nx) != len(self.ny):
+            raise ValueError("nx and ny differ in length")
+        self.n = len(self.nx)
+        self.order = order
+        self._h = C.c_void_p(None)
+        o = opts.to_c()
+        ax = (C.c_int * self.n)(*self.nx)
+        ay = (C.c_int * self.n)(*self.ny)
+        _check(_lib.mpdata_ensemble_create(C.byref(self._h), self.n, ax, ay, order, C.byref(o)))
+
+    def close(self):
+        if self._h and self._h.value:
+            _lib.mpdata_ensemble_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream_handle):
+        _check(_lib.mpdata_ensemble_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def set_faces(self, q, U, V):
+        (pu, w), (pv, _) = _ptr(U, np.float32), _ptr(V, np.float32)
+        _check(_lib.mpdata_ensemble_set_faces(self._h, q, pu, pv, w))
+
+    def set_field(self, q, c):
+        p, w = _ptr(c, np.float32)
+        _check(_lib.mpdata_ensemble_set_field(self._h, q, p, w))
+
+    def get_field(self, q, out=None):
+        if out is None:
+            out = np.empty((self.ny[q], self.nx[q]), np.float32)
+        p, w = _ptr(out, np.float32)
+        _check(_lib.mpdata_ensemble_get_field(self._h, q, p, w))
+        return out
+
+    def step(self, nsteps: int = 1, graph: bool = True):
+        fn = _lib.mpdata_ensemble_step if graph else _lib.mpdata_ensemble_step_direct
+        _check(fn(self._h, nsteps))
+
+    def sync(self):
+        _check(_lib.mpdata_ensemble_sync(self._h))
+
+    def autotune(self, trial_steps: int = 5):
+        t = C.c_int()
+        ms = C.c_double()
+        _check(_lib.mpdata_ensemble_autotune(self._h, trial_steps, C.byref(t), C.byref(ms)))
+        return t.value, ms.value
+
+    def set_tile(self, tile: int):
+        _check(_lib.mpdata_ensemble_tile(self._h, tile))

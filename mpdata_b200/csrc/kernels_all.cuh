@@ -8,6 +8,12 @@ namespace MPD_NS {
 
 #include "kernels_unfused.cuh"
 #include "kernels_fused.cuh"
+#include "kernels_ensemble.cuh"
+
+template int launch_ens_pass<float>(int, float*, const EnsInst*, const EnsItem*, int, int,
+                                    const EnsPass&, int, int, int, cudaStream_t);
+template int launch_ens_donor<float>(int, float*, const EnsInst*, const EnsItem*, int, int,
+                                     const EnsPass&, cudaStream_t);
 
 namespace {
 constexpr int kBX = 32, kBY = 8;

@@ -1,0 +1,300 @@
+// Batched ensemble of independent 2D problems: one launch per pass covers
+// every instance.
+//
+// An instance is a 2D grid nx x ny with a fixed one-cell shell: the
+// reference's 2D form is the 3D grid nx x ny x 3 with w = 0 (tests/init.c:64-68,
+// ring2d calls test_init(n, 3)); every z term there is an exact zero, so these
+// 2D formulas (the 3D ones with the z terms dropped, same evaluation order
+// otherwise) give the same values as the 3D kernels on the 3-plane form.
+//
+// Work list: (instance, tile) items over the instances' interior cells.  A
+// persistent grid of CTAs walks the list (item = blockIdx.x + n * gridDim.x);
+// per item the CTA stages the tile with a halo of 3 into shared memory with
+// coalesced loads, forms the faces (and, with the limiter, the ratios of the
+// tile plus a one-cell ring), and updates its cells.  Tile shape TX x TY is a
+// template parameter chosen by the host-side autotuner.
+//
+// Included by kernels_all.cuh inside namespace mpd::MPD_NS.
+
+namespace ens {
+
+constexpr int H = 3;  // staged halo (the y faces' divergent term reaches two x faces back)
+
+// The staged values the two high faces of one cell read (2D subset of Nb).
+template <typename T> struct Nb2 {
+    T C, L, R, D, Uu, RU, RD, LU;
+    T u, uL, uR, uL2, uLU, uU, uL2U;
+    T v, vD, vU, vR, vRD;
+};
+
+template <typename T> __device__ __forceinline__ Nb2<T> gather2(const T* c, const T* uo, const T* vo, int o, int Y)
+{
+    Nb2<T> n;
+    n.C = c[o]; n.L = c[o - 1]; n.R = c[o + 1]; n.D = c[o - Y]; n.Uu = c[o + Y];
+    n.RU = c[o + 1 + Y]; n.RD = c[o + 1 - Y]; n.LU = c[o - 1 + Y];
+    n.u = uo[o]; n.uL = uo[o - 1]; n.uR = uo[o + 1]; n.uL2 = uo[o - 2]; n.uLU = uo[o - 1 + Y];
+    n.uU = uo[o + Y]; n.uL2U = uo[o - 2 + Y];
+    n.v = vo[o]; n.vD = vo[o - Y]; n.vU = vo[o + Y]; n.vR = vo[o + 1]; n.vRD = vo[o + 1 - Y];
+    return n;
+}
+
+// x face between i and i+1 (uu.c:18-102 with the z terms, all zero here, dropped).
+template <bool AP, typename T>
+__device__ __forceinline__ T face_u2(const Nb2<T>& n, int i, int nx, int use_div)
+{
+    T vb, neg_div = T(0);
+    if (i == 0) {
+        vb = T(0.5) * (n.vRD + n.vR);
+    } else if (i == nx - 2) {
+        vb = T(0.5) * (n.vD + n.v);
+    } else {
+        vb = T(0.25) * (((n.vRD + n.vR) + n.v) + n.vD);
+        if (use_div) {
+            T s = n.uR - n.uL;
+            s = s + n.vRD;
+            s = s - n.vR;
+            s = s - n.v;
+            s = s + n.vD;
+            neg_div = -((T(0.25) * n.u) * s);
+        } else {
+            neg_div = -T(0);
+        }
+    }
+    T n1, d1;
+    grad_pair(n.RU, n.Uu, n.D, n.RD, n1, d1);
+    const T ma = mag(n.u);
+    const T t = neg_div + ratio<AP>((ma * (T(1) - ma)) * (n.R - n.C), (n.R + n.C) + tiny<T>());
+    return t - T(0.5) * (n.u * ratio<AP>(vb * n1, d1));
+}
+
+// y face between j and j+1 (vv.c:21-107, z terms dropped, column rule kept).
+template <bool AP, typename T>
+__device__ __forceinline__ T face_v2(const Nb2<T>& n, int i, int j, int ny, int use_div, int vv_fix,
+                                    int pass, T vadv)
+{
+    T ub, neg_div = T(0);
+    if (j == 0) {
+        ub = T(0.5) * (n.uLU + n.uU);
+    } else if (j == ny - 2) {
+        ub = T(0.5) * (n.uL + n.u);
+    } else {
+        if (i == 1 && !vv_fix) return (pass & 1) ? T(0) : vadv;  // vv.c:81-82
+        ub = T(0.25) * (((n.uLU + n.uU) + n.u) + n.uL);
+        if (use_div) {
+            const T ul2u = (i >= 2) ? n.uL2U : T(0);
+            const T ul2 = (i >= 2) ? n.uL2 : T(0);
+            T s = n.vU - n.vD;
+            s = s + n.uLU;
+            s = s - ul2u;
+            s = s - ul2;
+            s = s + n.uL;
+            neg_div = -((T(0.25) * n.v) * s);
+        } else {
+            neg_div = -T(0);
+        }
+    }
+    T n1, d1;
+    grad_pair(n.RU, n.R, n.L, n.LU, n1, d1);
+    const T ma = mag(n.v);
+    const T t = neg_div + ratio<AP>((ma * (T(1) - ma)) * (n.Uu - n.C), (n.Uu + n.C) + tiny<T>());
+    return t - T(0.5) * (n.v * ratio<AP>(ub * n1, d1));
+}
+
+}  // namespace ens
+
+// Donor-cell pass (smolar_pass.c:30-57, 2D), one thread per cell of a tile.
+template <typename T, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY)
+    k_ens_donor(T* __restrict__ arena, const EnsInst* __restrict__ insts,
+                const EnsItem* __restrict__ items, int nitems, EnsPass p)
+{
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const EnsItem item = items[it];
+        const EnsInst in = insts[item.inst];
+        const int i = item.i0 + threadIdx.x, j = item.j0 + threadIdx.y;
+        if (i > in.nx - 2 || j > in.ny - 2) continue;
+        const long long q = (long long)j * in.px + i;
+        const T* c0 = arena + in.c[p.in];
+        const T* U = arena + in.f[p.rs][0];
+        const T* V = arena + in.f[p.rs][1];
+        const T cc = c0[q];
+        const T fx = upwind(cc, c0[q + 1], U[q]) - upwind(c0[q - 1], cc, U[q - 1]);
+        const T fy = upwind(cc, c0[q + in.px], V[q]) - upwind(c0[q - in.px], cc, V[q - in.px]);
+        arena[in.c[p.out] + q] = cc - T(0.5) * (fx + fy);
+    }
+}
+
+// Corrective pass (antidiffusive faces + optional limiter + donor update), 2D.
+template <typename T, bool LIM, typename A, bool AP, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY)
+    k_ens_pass(T* __restrict__ arena, const EnsInst* __restrict__ insts,
+               const EnsItem* __restrict__ items, int nitems, EnsPass p)
+{
+    using namespace ens;
+    constexpr int SX = TX + 2 * H, SY = TY + 2 * H, PL = SX * SY;
+    constexpr int NT = TX * TY;
+    constexpr int OW = LIM ? 1 : 0;
+    constexpr int WX = TX + 2, WPL = WX * (TY + 2);  // work planes: local [-1, TX] x [-1, TY]
+    __shared__ T sC[PL], sU[PL], sV[PL], sN[LIM ? PL : 1];
+    __shared__ T sRU[WPL], sRV[WPL], sBU[LIM ? WPL : 1], sBD[LIM ? WPL : 1];
+    const int x = threadIdx.x, y = threadIdx.y, tid = y * TX + x;
+    const int o = (y + H) * SX + (x + H);
+    const int w = (y + 1) * WX + (x + 1);
+    const bool ex_u = tid < TY, ex_v = tid >= TY && tid < TY + TX;
+
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const EnsItem item = items[it];
+        const EnsInst in = insts[item.inst];
+        const int nx = in.nx, ny = in.ny, px = in.px;
+        const int i0 = item.i0 - OW, j0 = item.j0 - OW;  // global cell of local (0, 0)
+        const T* gc = arena + in.c[p.in];
+        const T* gn = arena + in.c[p.cn];
+        const T* gu = arena + in.f[p.rs][0];
+        const T* gv = arena + in.f[p.rs][1];
+        const T* vadv = arena + in.f[0][1];
+        __syncthreads();  // the previous item's reads of the stage are done
+        for (int e = tid; e < PL; e += NT) {
+            const int sy = e / SX, sx = e - sy * SX;
+            const int gi = i0 - H + sx, gj = j0 - H + sy;
+            const bool inside = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
+            const long long q = (long long)gj * px + gi;
+            sC[e] = inside ? gc[q] : T(0);
+            sU[e] = inside ? gu[q] : T(0);
+            sV[e] = inside ? gv[q] : T(0);
+            if (LIM) sN[e] = inside ? gn[q] : T(0);
+        }
+        __syncthreads();
+
+        const int i = i0 + x, j = j0 + y;
+        const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
+        const bool owned = cell_in && (!LIM || (x >= 1 && x <= TX - 2 && y >= 1 && y <= TY - 2));
+        T ru = T(0), rv = T(0);
+        {
+            const Nb2<T> nb = gather2(sC, sU, sV, o, SX);
+            if (i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2) ru = face_u2<AP>(nb, i, nx, p.use_div);
+            if (i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2) {
+                const T va = (i == 1) ? vadv[(long long)j * px + 1] : T(0);
+                rv = face_v2<AP>(nb, i, j, ny, p.use_div, p.vv_fix, p.pass, va);
+            }
+        }
+        sRU[w] = ru;
+        sRV[w] = rv;
+        if (ex_u || ex_v) {  // faces just below the tile
+            const int ei = ex_u ? i0 - 1 : i0 + (tid - TY);
+            const int ej = ex_u ? j0 + tid : j0 - 1;
+            const int eo = (ej - j0 + H) * SX + (ei - i0 + H);
+            T ev = T(0);
+            const Nb2<T> nb = gather2(sC, sU, sV, eo, SX);
+            if (ex_u && ei >= 0 && ei <= nx - 2 && ej >= 1 && ej <= ny - 2)
+                ev = face_u2<AP>(nb, ei, nx, p.use_div);
+            if (ex_v && ei >= 1 && ei <= nx - 2 && ej >= 0 && ej <= ny - 2) {
+                const T va = (ei == 1) ? vadv[(long long)ej * px + 1] : T(0);
+                ev = face_v2<AP>(nb, ei, ej, ny, p.use_div, p.vv_fix, p.pass, va);
+            }
+            if (ex_u) sRU[(tid + 1) * WX] = ev;
+            else sRV[tid - TY + 1] = ev;
+        }
+        __syncthreads();
+
+        T ur = ru, ul = sRU[w - 1], vt = rv, vb = sRV[w - WX];
+        if (LIM) {
+            T bu = T(1), bd = T(1);
+            if (cell_in) {
+                const T psi = sC[o], cl = sC[o - 1], cr = sC[o + 1], cd = sC[o - SX], cu = sC[o + SX];
+                T mx = vmax(psi, sN[o]), mn = vmin(psi, sN[o]);
+                mx = vmax(vmax(cl, sN[o - 1]), mx); mn = vmin(vmin(cl, sN[o - 1]), mn);
+                mx = vmax(vmax(cr, sN[o + 1]), mx); mn = vmin(vmin(cr, sN[o + 1]), mn);
+                mx = vmax(vmax(cd, sN[o - SX]), mx); mn = vmin(vmin(cd, sN[o - SX]), mn);
+                mx = vmax(vmax(cu, sN[o + SX]), mx); mn = vmin(vmin(cu, sN[o + SX]), mn);
+                A fin = A(0), fout = A(0);
+                lim_acc(lim_flux<T, A>(ul, cl, psi), false, fin, fout);
+                lim_acc(lim_flux<T, A>(ru, psi, cr), true, fin, fout);
+                lim_acc(lim_flux<T, A>(vb, cd, psi), false, fin, fout);
+                lim_acc(lim_flux<T, A>(rv, psi, cu), true, fin, fout);
+                bu = T(ratio<AP>(A(mx) - A(psi), fin + lim_tiny<A>()));
+                bd = T(ratio<AP>(A(psi) - A(mn), fout + lim_tiny<A>()));
+            }
+            sBU[w] = bu;
+            sBD[w] = bd;
+            __syncthreads();
+            auto BU = [&](int q2) { return sBU[q2]; };
+            auto BD = [&](int q2) { return sBD[q2]; };
+            if (owned) {
+                ur = limit_face(ru, BU(w), BD(w), BU(w + 1), BD(w + 1));
+                ul = limit_face(ul, BU(w - 1), BD(w - 1), BU(w), BD(w));
+                vt = limit_face(rv, BU(w), BD(w), BU(w + WX), BD(w + WX));
+                vb = limit_face(vb, BU(w - WX), BD(w - WX), BU(w), BD(w));
+            }
+        }
+        if (owned) {
+            const long long q = (long long)j * px + i;
+            const T cc = sC[o];
+            const T fx = upwind(cc, sC[o + 1], ur) - upwind(sC[o - 1], cc, ul);
+            const T fy = upwind(cc, sC[o + SX], vt) - upwind(sC[o - SX], cc, vb);
+            arena[in.c[p.out] + q] = cc - T(0.5) * (fx + fy);
+            if (p.write_faces) {
+                arena[in.f[p.ws][0] + q] = ur;
+                arena[in.f[p.ws][1] + q] = vt;
+                if (i == 1) arena[in.f[p.ws][0] + q - 1] = ul;
+                if (j == 1) arena[in.f[p.ws][1] + q - px] = vb;
+            }
+        }
+    }
+}
+
+template <typename T, bool LIM, typename A, bool AP, int TX, int TY>
+void ens_launch_pass(T* arena, const EnsInst* insts, const EnsItem* items, int nitems, int grid,
+                     const EnsPass& p, cudaStream_t s)
+{
+    k_ens_pass<T, LIM, A, AP, TX, TY><<<grid, dim3(TX, TY), 0, s>>>(arena, insts, items, nitems, p);
+}
+
+template <typename T, int TX, int TY>
+void ens_launch_donor_t(T* arena, const EnsInst* insts, const EnsItem* items, int nitems, int grid,
+                        const EnsPass& p, cudaStream_t s)
+{
+    k_ens_donor<T, TX, TY><<<grid, dim3(TX, TY), 0, s>>>(arena, insts, items, nitems, p);
+}
+
+// Dispatch on the runtime tile index (the autotuner's candidates) and options.
+template <typename T, int TX, int TY>
+void ens_pass_tile(T* arena, const EnsInst* insts, const EnsItem* items, int nitems, int grid,
+                   const EnsPass& p, int limiter, int wide, int approx, cudaStream_t s)
+{
+    if (!limiter) {
+        if (approx) ens_launch_pass<T, false, T, true, TX, TY>(arena, insts, items, nitems, grid, p, s);
+        else ens_launch_pass<T, false, T, false, TX, TY>(arena, insts, items, nitems, grid, p, s);
+    } else if (wide) {
+        if (approx) ens_launch_pass<T, true, double, true, TX, TY>(arena, insts, items, nitems, grid, p, s);
+        else ens_launch_pass<T, true, double, false, TX, TY>(arena, insts, items, nitems, grid, p, s);
+    } else {
+        if (approx) ens_launch_pass<T, true, T, true, TX, TY>(arena, insts, items, nitems, grid, p, s);
+        else ens_launch_pass<T, true, T, false, TX, TY>(arena, insts, items, nitems, grid, p, s);
+    }
+}
+
+template <typename T>
+int launch_ens_pass(int tile, T* arena, const EnsInst* insts, const EnsItem* items, int nitems,
+                    int grid, const EnsPass& p, int limiter, int wide, int approx, cudaStream_t s)
+{
+    switch (tile) {
+    case 0: ens_pass_tile<T, 32, 8>(arena, insts, items, nitems, grid, p, limiter, wide, approx, s); break;
+    case 1: ens_pass_tile<T, 32, 16>(arena, insts, items, nitems, grid, p, limiter, wide, approx, s); break;
+    case 2: ens_pass_tile<T, 64, 8>(arena, insts, items, nitems, grid, p, limiter, wide, approx, s); break;
+    default: return -1;
+    }
+    return 0;
+}
+
+template <typename T>
+int launch_ens_donor(int tile, T* arena, const EnsInst* insts, const EnsItem* items, int nitems,
+                     int grid, const EnsPass& p, cudaStream_t s)
+{
+    switch (tile) {
+    case 0: ens_launch_donor_t<T, 32, 8>(arena, insts, items, nitems, grid, p, s); break;
+    case 1: ens_launch_donor_t<T, 32, 16>(arena, insts, items, nitems, grid, p, s); break;
+    case 2: ens_launch_donor_t<T, 64, 8>(arena, insts, items, nitems, grid, p, s); break;
+    default: return -1;
+    }
+    return 0;
+}

@@ -49,7 +49,34 @@ template <typename T> struct PassArgs {
     int approx;        // fused FP32 path: hardware-reciprocal ratios (approx_div form)
 };
 
+// Ensemble (batched 2D instances): per-instance descriptor with the element
+// offsets of its arrays inside the ensemble's arena.
+struct EnsInst {
+    int nx, ny, px, pad;
+    long long c[3];     // field levels
+    long long f[3][2];  // face sets: [0] advective, [1..2] Jacobi ping-pong; [axis] U, V
+};
+
+// One work item: a tile of an instance, given by its first interior cell.
+struct EnsItem {
+    int inst, i0, j0, pad;
+};
+
+// Which levels / face sets a pass reads and writes (the same for every instance).
+struct EnsPass {
+    int in, out, cn;   // field levels
+    int rs, ws;        // face sets read / written
+    int pass, use_div, vv_fix, write_faces;
+};
+
 #define MPD_DECLARE_LAUNCHERS                                                              \
+    template <typename T>                                                                  \
+    int launch_ens_pass(int tile, T* arena, const EnsInst* insts, const EnsItem* items,    \
+                        int nitems, int grid, const EnsPass& p, int limiter, int wide,     \
+                        int approx, cudaStream_t s);                                       \
+    template <typename T>                                                                  \
+    int launch_ens_donor(int tile, T* arena, const EnsInst* insts, const EnsItem* items,   \
+                         int nitems, int grid, const EnsPass& p, cudaStream_t s);          \
     template <typename T>                                                                  \
     void launch_courant(const Dims& d, const T* dx, const T* dy, const T* ds, T dt,        \
                         const T* u0, const T* u1, const T* v0, const T* v1, const T* w0,   \

@@ -144,3 +144,32 @@ def random_case(nx, ny, ns, seed=0, courant=0.3, positive=True):
     c = rng.uniform(0.0, 1.0, sh) if positive else rng.uniform(-1.0, 1.0, sh)
     dx = rng.uniform(0.8, 1.2, nx); dy = rng.uniform(0.8, 1.2, ny); ds = rng.uniform(0.8, 1.2, ns)
     return dict(u0=u0, u1=u1, v0=v0, v1=v1, w0=w0, w1=w1, c0=c, dx=dx, dy=dy, ds=ds, dt=0.9)
+
+
+def ensemble(n: int = 256, lo: int = 64, hi: int = 512, seed: int = SEED + 4):
+    """Batched-ensemble configuration: n independent 2D instances, NX, NY
+    uniform in [lo, hi], solid-body rotation with max Courant uniform in
+    [0.2, 0.5], Gaussian blob (sigma 4-16 cells, centre at least 3 sigma from
+    the edges), IORD 2 with the limiter.  Returns a list of dicts with 2D
+    faces U, V (float64) and field c0, shape (ny, nx)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx = int(rng.integers(lo, hi + 1)); ny = int(rng.integers(lo, hi + 1))
+        cour = rng.uniform(0.2, 0.5)
+        sig = rng.uniform(4.0, 16.0)
+        sig = min(sig, (min(nx, ny) - 3) / 6.0 - 1e-3)
+        cx = rng.uniform(3 * sig, nx - 1 - 3 * sig)
+        cy = rng.uniform(3 * sig, ny - 1 - 3 * sig)
+        yc, xc = (ny - 1) / 2.0, (nx - 1) / 2.0
+        y, x = np.mgrid[0:ny, 0:nx].astype(np.float64)
+        U = np.zeros((ny, nx)); V = np.zeros((ny, nx))
+        # faces of interior rows/columns; boundary faces zero (closed box)
+        U[1:-1, 1:-1] = -(y[1:-1, 1:-1] - yc)
+        V[1:-1, 1:-1] = (x[1:-1, 1:-1] - xc)
+        U[:, 0] = 0.0; U[:, -1] = 0.0; U[:, -2] = 0.0
+        V[0, :] = 0.0; V[-1, :] = 0.0; V[-2, :] = 0.0
+        s = cour / max(np.abs(U).max(), np.abs(V).max())
+        c0 = np.exp(-0.5 * ((x - cx) ** 2 + (y - cy) ** 2) / sig ** 2)
+        out.append(dict(nx=nx, ny=ny, U=U * s, V=V * s, c0=c0))
+    return out
