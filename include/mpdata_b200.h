@@ -225,6 +225,31 @@ int mpdata_ensemble_autotune(mpdata_ensemble_handle e, int trial_steps, int* cho
 /* Force a tile-shape candidate (0: 32x8, 1: 32x16, 2: 64x8 threads). */
 int mpdata_ensemble_tile(mpdata_ensemble_handle e, int tile);
 
+/* ---- Adjoint of a window of steps ------------------------------------------
+ *
+ * No reference counterpart.  Hand-written reverse mode of the full step
+ * (donor pass, antidiffusive passes, limiter) with every branch frozen at its
+ * forward choice (sign of each face value in |U|, the limiter's min
+ * selections and the argmax/argmin of its bounds).  Steady faces; the
+ * adjoint is taken with respect to the field.
+ *
+ * mpdata_adjoint_forward steps c0 through nsteps steps (cN receives the
+ * result if non-NULL), storing a checkpoint every `checkpoint_every` steps;
+ * mpdata_adjoint_backward maps the adjoint of the window's output (lamN) to
+ * the adjoint of its input (lam0), recomputing each checkpoint segment.
+ * Arrays as in mpdata_set_field (full grids, dense, host or device). */
+typedef struct mpdata_adjoint* mpdata_adjoint_handle;
+
+int mpdata_adjoint_create(mpdata_adjoint_handle* h, int nx, int ny, int ns, int dtype, int order,
+                          const struct mpdata_options* opts, int checkpoint_every);
+int mpdata_adjoint_destroy(mpdata_adjoint_handle h);
+int mpdata_adjoint_set_stream(mpdata_adjoint_handle h, void* stream);
+int mpdata_adjoint_set_faces(mpdata_adjoint_handle h, const void* U, const void* V,
+                             const void* W, int where);
+int mpdata_adjoint_forward(mpdata_adjoint_handle h, const void* c0, int nsteps, void* cN,
+                           int where);
+int mpdata_adjoint_backward(mpdata_adjoint_handle h, const void* lamN, void* lam0, int where);
+
 /* ---- 3. Allocation-free step --------------------------------------------
  *
  * No counterpart in the reference.  One FP32 step (`order` passes, optional

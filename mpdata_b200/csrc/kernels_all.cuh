@@ -9,6 +9,39 @@ namespace MPD_NS {
 #include "kernels_unfused.cuh"
 #include "kernels_fused.cuh"
 #include "kernels_ensemble.cuh"
+#include "kernels_adjoint.cuh"
+
+// Corrective pass with its intermediates kept for the adjoint: the raw faces
+// go to R, the limited faces to a.Un/Vn/Wn (copied from R and limited in place).
+template <typename T>
+void launch_pass_record(const Dims& d, const PassArgs<T>& a, T* RU, T* RV, T* RW, T* bup, T* bdn,
+                        cudaStream_t s)
+{
+    dim3 g((d.nx + 31) / 32, (d.ny + 7) / 8, d.ns), b(32, 8);
+    k_antidiff<T><<<g, b, 0, s>>>(d, a.c, a.Uo, a.Vo, a.Wo, a.Vadv, RU, RV, RW, a.pass, a.use_div,
+                                  a.vv_fix);
+    const size_t fb = (size_t)d.pp * d.ns * sizeof(T);
+    if (a.limiter) {
+        if (a.wide)
+            k_fct_beta<T, double><<<g, b, 0, s>>>(d, a.c, a.cn, RU, RV, RW, bup, bdn);
+        else
+            k_fct_beta<T, T><<<g, b, 0, s>>>(d, a.c, a.cn, RU, RV, RW, bup, bdn);
+        cudaMemcpyAsync(a.Un, RU, fb, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(a.Vn, RV, fb, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(a.Wn, RW, fb, cudaMemcpyDeviceToDevice, s);
+        k_fct_apply<T><<<g, b, 0, s>>>(d, bup, bdn, a.Un, a.Vn, a.Wn);
+        k_donor<T><<<g, b, 0, s>>>(d, a.c, a.Un, a.Vn, a.Wn, a.c_out, 1);
+    } else {
+        k_donor<T><<<g, b, 0, s>>>(d, a.c, RU, RV, RW, a.c_out, 1);
+    }
+}
+
+template void launch_pass_record<float>(const Dims&, const PassArgs<float>&, float*, float*, float*,
+                                        float*, float*, cudaStream_t);
+template void launch_pass_record<double>(const Dims&, const PassArgs<double>&, double*, double*,
+                                         double*, double*, double*, cudaStream_t);
+template void launch_adj_pass<float>(const Dims&, const AdjPassArgs<float>&, cudaStream_t);
+template void launch_adj_pass<double>(const Dims&, const AdjPassArgs<double>&, cudaStream_t);
 
 template int launch_ens_pass<float>(int, float*, const EnsInst*, const EnsItem*, int, int,
                                     const EnsPass&, int, int, int, cudaStream_t);

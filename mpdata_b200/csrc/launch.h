@@ -69,7 +69,31 @@ struct EnsPass {
     int pass, use_div, vv_fix, write_faces;
 };
 
+// Adjoint of one pass o of a step (kernels_adjoint.cuh).
+template <typename T> struct AdjPassArgs {
+    int pass, limiter, wide, use_div, vv_fix;
+    const T *c, *cn;               // level c_o, step input c_0
+    const T *FU, *FV, *FW;         // faces of this pass's donor update (advective for o = 0)
+    const T *RU, *RV, *RW;         // raw antidiffusive faces of pass o
+    const T *bup, *bdn;            // limiter ratios of pass o
+    const T *Uo, *Vo, *Wo;         // previous faces (the pattern's inputs)
+    const T* lam_out;              // adjoint of c_{o+1}
+    T* lam_in;                     // adjoint of c_o (+=)
+    T* lam_cn;                     // adjoint of c_0 (+=, limiter bounds)
+    T *lFU, *lFV, *lFW;            // adjoint of this pass's donor faces (+=; null for o = 0)
+    T *lRU, *lRV, *lRW;            // adjoint of the raw faces (+=; limiter only)
+    T *lbup, *lbdn;                // adjoint of the ratios (+=)
+    T *lUo, *lVo, *lWo;            // adjoint of the previous faces (+=; null if advective)
+};
+
 #define MPD_DECLARE_LAUNCHERS                                                              \
+    template <typename T> void launch_adj_pass(const Dims& d, const AdjPassArgs<T>& a,      \
+                                               cudaStream_t s);                            \
+    /* Corrective pass keeping its intermediates: raw faces R, limited faces L (= R         \
+       without limiter, may alias), ratios bup/bdn. */                                     \
+    template <typename T>                                                                  \
+    void launch_pass_record(const Dims& d, const PassArgs<T>& a, T* RU, T* RV, T* RW,       \
+                            T* bup, T* bdn, cudaStream_t s);                               \
     template <typename T>                                                                  \
     int launch_ens_pass(int tile, T* arena, const EnsInst* insts, const EnsItem* items,    \
                         int nitems, int grid, const EnsPass& p, int limiter, int wide,     \
