@@ -324,6 +324,9 @@ def run_gpu(args):
     ens = None
     if rank == 0 and not args.no_ensemble:
         ens = run_ensemble(m, torch, args.ensemble_steps, 10)
+    adj = None
+    if rank == 0 and not args.no_adjoint:
+        adj = run_adjoint(m, torch)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -371,6 +374,8 @@ def run_gpu(args):
         line["e2e"] = e2e
     if ens:
         line["ensemble"] = ens
+    if adj:
+        line["adjoint"] = adj
     if world == 1 and not args.no_cpu:
         cb = cpu_reference(steps=2, warmup=1)
         if cb:
@@ -447,6 +452,101 @@ def run_ensemble(m, torch, steps: int, base_steps: int):
             "min_interior_value": min(mins)}
 
 
+def run_adjoint(m, torch, nsteps: int = 200, every: int = 20, ndir: int = 32):
+    """Adjoint source-inversion configuration: 128x128x64, ring3d-type flow,
+    IORD 2 + limiter (branches frozen), FP32 forward and adjoint, window of
+    200 steps with a checkpoint every 20, loss = sum of squared differences at
+    64 seeded receptors against a target from a different blob.  Reports the
+    reverse sweep's cost per step against a forward step (the fused
+    production step and the recording forward the adjoint replays), and the
+    gradient's agreement with FP64 central differences along 32 random
+    directions and with the FP64 adjoint."""
+    import mpdata_b200.adjoint as ma
+    from mpdata_b200 import workloads
+    n, ns = 128, 64
+    r = workloads.ring3d(n=n, ns=ns, courant=0.4, wcourant=0.1, sigma=6.0, offset=30.0,
+                         background=1e-6)
+    tr = workloads.ring3d(n=n, ns=ns, courant=0.4, wcourant=0.1, sigma=8.0, offset=-25.0,
+                          background=1e-6)["c0"]
+    faces = workloads.faces_from_cells(r["u"], r["v"], r["w"])
+    k, j, i = np.mgrid[0:ns, 0:n, 0:n].astype(np.float64)
+    # smoothly varying background: no exactly uniform region (where the
+    # limiter ratio is 0/0 and the frozen-branch derivative is not defined)
+    c0 = r["c0"] + 1e-4 * (1.5 + np.sin(0.3 * i) * np.cos(0.25 * j + 0.2 * k))
+    rng = np.random.default_rng(workloads.SEED + 5)
+    rec = rng.integers(0, c0.size, 64)
+    t_rec = tr.reshape(-1)[rec]
+
+    def lam_of(cN):
+        lam = np.zeros(c0.size)
+        np.add.at(lam, rec, 2.0 * (cN.reshape(-1)[rec] - t_rec))
+        return lam.reshape(c0.shape)
+
+    def loss_of(cN):
+        return float(np.sum((cN.reshape(-1)[rec] - t_rec) ** 2))
+
+    out = {"grid": [n, n, ns], "steps": nsteps, "checkpoint_every": every, "receptors": 64}
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+    grads = {}
+    for dt in (np.float32, np.float64):
+        a = ma.Adjoint(n, n, ns, order=2, dtype=dt, checkpoint_every=every, limiter=True)
+        a.set_stream(stream.cuda_stream)
+        a.set_faces(*(np.ascontiguousarray(f, dt) for f in faces))
+        cd = np.ascontiguousarray(c0, dt)
+        a.forward(cd, nsteps)  # warm-up
+        ev0.record(stream)
+        cN = a.forward(cd, nsteps)
+        ev1.record(stream)
+        ev1.synchronize()
+        t_f = ev0.elapsed_time(ev1)
+        lam = np.ascontiguousarray(lam_of(cN.astype(np.float64)), dt)
+        ev0.record(stream)
+        g = a.backward(lam)
+        ev1.record(stream)
+        ev1.synchronize()
+        t_b = ev0.elapsed_time(ev1)
+        grads[np.dtype(dt).name] = g.astype(np.float64)
+        if dt is np.float32:
+            out["t_fwd_recording_ms_per_step"] = t_f / nsteps
+            out["t_adj_ms_per_step"] = t_b / nsteps
+        a.close()
+    # production forward step (fused kernels) on the same problem
+    s = m.Solver(n, n, ns, order=2, limiter=True)
+    s.set_stream(stream.cuda_stream)
+    s.set_faces(*(np.ascontiguousarray(f, np.float32) for f in faces))
+    s.set_field(np.ascontiguousarray(c0, np.float32))
+    s.step(5)
+    ev0.record(stream)
+    s.step(nsteps)
+    ev1.record(stream)
+    ev1.synchronize()
+    out["t_fwd_fused_ms_per_step"] = ev0.elapsed_time(ev1) / nsteps
+    s.close()
+    out["t_adj_over_t_fwd_fused"] = out["t_adj_ms_per_step"] / out["t_fwd_fused_ms_per_step"]
+    out["t_adj_over_t_fwd_recording"] = out["t_adj_ms_per_step"] / out["t_fwd_recording_ms_per_step"]
+    g32, g64 = grads["float32"], grads["float64"]
+    out["fp32_vs_fp64_adjoint_rel_l2"] = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+    # central differences of the FP64 window along random directions
+    a64 = ma.Adjoint(n, n, ns, order=2, dtype=np.float64, checkpoint_every=every, limiter=True)
+    a64.set_faces(*(np.ascontiguousarray(f, np.float64) for f in faces))
+    errs = []
+    for _ in range(ndir):
+        v = rng.standard_normal(c0.shape) * c0 * 1e-3
+        e = 1e-3
+        lp = loss_of(a64.forward(np.ascontiguousarray(c0 + e * v), nsteps))
+        lm = loss_of(a64.forward(np.ascontiguousarray(c0 - e * v), nsteps))
+        fd = (lp - lm) / (2 * e)
+        ad = float(np.sum(g32 * v))
+        errs.append(abs(fd - ad) / max(abs(fd), 1e-30))
+    a64.close()
+    out["fd_directions"] = ndir
+    out["fd_max_rel_err_fp32_adjoint"] = max(errs)
+    out["fd_median_rel_err_fp32_adjoint"] = float(np.median(errs))
+    return out
+
+
 def run_e2e(m, args, form_opts):
     """Same workload through smolar() (the drop-in entry point) with pinned
     host arrays; per step: upload of the 3 distinct velocity arrays + field,
@@ -518,6 +618,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=500)
     ap.add_argument("--size", default=None,
                     help="nx,ny,ns override (profiling captures of a smaller grid only)")

@@ -183,6 +183,16 @@ int mpdata_min(mpdata_handle h, double* minval, long long* nneg);
 /* Kernel launches a single mpdata_step(h, 1) issues. */
 int mpdata_launches_per_step(mpdata_handle h);
 
+/* z-march depth of the fused kernels: each CTA marches a chunk of `depth`
+ * interior planes (after a 2-3 plane warm-up that keeps results identical);
+ * 0 = the whole column.  A default is chosen at creation from the grid size;
+ * mpdata_autotune times the candidates (whole, 128, 64, 32, 16, 8) over
+ * trial_steps steps on the handle's own field, keeps the fastest and puts
+ * the field back as it was. */
+int mpdata_set_march_depth(mpdata_handle h, int depth);
+int mpdata_march_depth(mpdata_handle h);
+int mpdata_autotune(mpdata_handle h, int trial_steps, int* depth, double* ms_per_step);
+
 /* Per-pass kernel timing with CUDA events on the handle's stream (for the
  * roofline report).  While enabled, every mpdata_step records an event pair
  * around the donor pass and around each corrective pass.  mpdata_pass_times

@@ -90,6 +90,9 @@ _lib.mpdata_ensemble_step_direct.argtypes = [_vp, C.c_int]
 _lib.mpdata_ensemble_sync.argtypes = [_vp]
 _lib.mpdata_ensemble_autotune.argtypes = [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
 _lib.mpdata_ensemble_tile.argtypes = [_vp, C.c_int]
+_lib.mpdata_set_march_depth.argtypes = [_vp, C.c_int]
+_lib.mpdata_march_depth.argtypes = [_vp]
+_lib.mpdata_autotune.argtypes = [_vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
 _lib.mpdata_enable_pass_timing.argtypes = [_vp, C.c_int]
 _lib.mpdata_pass_times.argtypes = [_vp, C.POINTER(C.c_double * 3), C.POINTER(C.c_longlong * 3),
                                    C.c_int]
@@ -330,6 +333,20 @@ class Solver:
 
     def launches_per_step(self) -> int:
         return _check(_lib.mpdata_launches_per_step(self._h))
+
+    def set_march_depth(self, depth: int):
+        _check(_lib.mpdata_set_march_depth(self._h, depth))
+
+    def march_depth(self) -> int:
+        return _check(_lib.mpdata_march_depth(self._h))
+
+    def autotune(self, trial_steps: int = 5):
+        """Time the z-march depth candidates on this solver's field, keep the
+        fastest; returns (depth, ms per step).  The field is restored."""
+        dep = C.c_int()
+        ms = C.c_double()
+        _check(_lib.mpdata_autotune(self._h, trial_steps, C.byref(dep), C.byref(ms)))
+        return dep.value, ms.value
 
     def enable_pass_timing(self, on: bool = True):
         _check(_lib.mpdata_enable_pass_timing(self._h, int(on)))

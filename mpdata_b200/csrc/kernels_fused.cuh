@@ -293,30 +293,39 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
         return reinterpret_cast<const T*>(smem + (size_t)(s * NARR + arr) * SB);
     };
 
+    // z chunk: this CTA updates planes [z0, z1); the march starts a few planes
+    // earlier so every value the first updated plane reads is formed exactly
+    // as an unchunked march would form it (2 planes of warm-up without the
+    // limiter, 3 with it: the z faces below, then the ratios below).
+    const int depth = a.zdepth > 0 ? a.zdepth : ns - 2;
+    const int z0 = 1 + (int)blockIdx.z * depth;
+    const int z1 = min(ns - 1, z0 + depth);
+    const int kstart = max(0, z0 - (LIM ? 3 : 2));
+    const int last = LIM ? z1 : z1 - 1;  // iteration of the last update
+
     bool ok = true;
-    int confirmed = 0;  // planes whose stage thread 0 has seen complete
+    int confirmed = kstart;  // planes below this one: thread 0 has seen their stage complete
     if (tid == 0) {
-        issue(0);
-        issue(1);
+        issue(kstart);
+        issue(kstart + 1);
     }
-    ok = tma::mbar_wait(&bars[0], 0);
-    if (tid == 0 && ok) confirmed = 1;
+    ok = tma::mbar_wait(&bars[kstart & (NSTAGE - 1)], 0);
+    if (tid == 0 && ok) confirmed = kstart + 1;
 
     // Register state carried between planes.
-    T cq0 = T(0), cq1 = T(0), cq2 = ok ? box(0, 0)[o] : T(0), cq3 = T(0);  // own c, planes k-2..k+1
+    T cq0 = T(0), cq1 = T(0), cq2 = ok ? box(kstart, 0)[o] : T(0), cq3 = T(0);  // own c, planes k-2..k+1
     T rw_prev = T(0);                      // raw z face below (face-plane k-1)
     T bu_prev = T(1), bd_prev = T(1);      // own ratios of plane k-1
     T lu_prev = T(0), lv_prev = T(0), lw_prev = T(0);  // limited faces of plane k-1 / face-plane k-2
 
-    const int last = LIM ? ns - 1 : ns - 2;
     // One plane of the march; S = k mod NSTAGE (compile-time).
     auto plane = [&](auto Sc, const int k) {
         constexpr int S = decltype(Sc)::value;
         constexpr int SM1 = (S + NSTAGE - 1) % NSTAGE, SP1 = (S + 1) % NSTAGE, SP2 = (S + 2) % NSTAGE;
         __syncthreads();  // every read of the slot plane k+2 reuses is done
-        if (tid == 0 && k + 2 <= ns - 1) issue(k + 2);
+        if (tid == 0 && k + 2 <= min(ns - 1, last + 1)) issue(k + 2);
         if (k + 1 <= ns - 1) {
-            if (ok) ok = tma::mbar_wait(&bars[SP1], ((k + 1) / NSTAGE) & 1);
+            if (ok) ok = tma::mbar_wait(&bars[SP1], ((k + 1 - kstart) / NSTAGE) & 1);
             if (tid == 0 && ok) confirmed = k + 2;
             cq3 = slot(SP1, 0)[o];
         }
@@ -393,14 +402,16 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
             if (a.write_faces) {
                 const bool ox = x >= 1 && x <= BX - 2, oy = y >= 1 && y <= BY - 2;
                 const long long q = cell(d, i, j, k);
-                if (kin && u_ok && oy && (ox || i == 0)) a.Un[q] = lu;
-                if (kin && v_ok && ox && (oy || j == 0)) a.Vn[q] = lv;
-                if (k >= 1 && owned) a.Wn[q - d.pp] = lw;
+                const bool mine_k = k >= z0 && k < z1;  // this chunk's planes
+                if (kin && mine_k && u_ok && oy && (ox || i == 0)) a.Un[q] = lu;
+                if (kin && mine_k && v_ok && ox && (oy || j == 0)) a.Vn[q] = lv;
+                // face-plane k-1: the high face of plane k-1, and face-plane 0 in the first chunk
+                if (k >= 1 && owned && k - 1 < z1 && (k - 1 >= z0 || k - 1 == 0)) a.Wn[q - d.pp] = lw;
             }
 
             // ---- donor update of plane k-1 ----
             const int u = k - 1;
-            if (u >= 1 && u <= ns - 2 && owned) {
+            if (u >= z0 && u < z1 && owned) {
                 const T* cu = slot(SM1, 0);
                 const T ul = sLU[(SM1 & 1) * WPL + w - 1];
                 const T vb = sLV[(SM1 & 1) * WPL + w - WX];
@@ -415,7 +426,7 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
             bd_prev = bd;
         } else {
             // ---- donor update of plane k ----
-            if (kin && owned) {
+            if (k >= z0 && k < z1 && owned) {
                 const T* c0 = slot(S, 0);
                 const T ul = sRU[w - 1], vb = sRV[w - WX];
                 const long long q = cell(d, i, j, k);
@@ -436,17 +447,18 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
         cq1 = cq2;
         cq2 = cq3;
     };
-    for (int kb = 0; kb <= last; kb += NSTAGE) {
-        plane(IC<0>{}, kb);
-        if (kb + 1 <= last) plane(IC<1>{}, kb + 1);
-        if (kb + 2 <= last) plane(IC<2>{}, kb + 2);
-        if (kb + 3 <= last) plane(IC<3>{}, kb + 3);
+    for (int kb = kstart & ~(NSTAGE - 1); kb <= last; kb += NSTAGE) {
+        if (kb >= kstart) plane(IC<0>{}, kb);
+        if (kb + 1 >= kstart && kb + 1 <= last) plane(IC<1>{}, kb + 1);
+        if (kb + 2 >= kstart && kb + 2 <= last) plane(IC<2>{}, kb + 2);
+        if (kb + 3 >= kstart && kb + 3 <= last) plane(IC<3>{}, kb + 3);
     }
 
     if (!ok && a.err) atomicOr(a.err, 1);
     if (tid == 0) {  // never leave with a copy in flight
-        for (int p = confirmed; p <= ns - 1 && p <= last + 1; p++)
-            if (!tma::mbar_wait(&bars[p & (NSTAGE - 1)], (p / NSTAGE) & 1)) break;
+        const int issued_last = min(ns - 1, last + 1);
+        for (int p = confirmed; p <= issued_last; p++)
+            if (!tma::mbar_wait(&bars[p & (NSTAGE - 1)], ((p - kstart) / NSTAGE) & 1)) break;
     }
 }
 
@@ -462,7 +474,9 @@ int launch_fused_variant(const Dims& d, const PassArgs<T>& a, cudaStream_t s)
         configured = true;
     }
     constexpr int OW = LIM ? 1 : 0;
-    dim3 g((d.nx - 2 + BX - 2 * OW - 1) / (BX - 2 * OW), (d.ny - 2 + BY - 2 * OW - 1) / (BY - 2 * OW));
+    const int depth = a.zdepth > 0 ? a.zdepth : d.ns - 2;
+    dim3 g((d.nx - 2 + BX - 2 * OW - 1) / (BX - 2 * OW), (d.ny - 2 + BY - 2 * OW - 1) / (BY - 2 * OW),
+           (d.ns - 2 + depth - 1) / depth);
     dim3 b(BX, BY);
     const CUtensorMap& cn = LIM ? *a.maps.cn : *a.maps.c;
     k_pass_tma<T, LIM, A, AP><<<g, b, smem, s>>>(d, a, *a.maps.c, cn, *a.maps.uo, *a.maps.vo,

@@ -47,6 +47,7 @@ template <typename T> struct PassArgs {
     int wide;          // FP64 limiter ratios (float storage only)
     int write_faces;   // the next pass reads Un/Vn/Wn
     int approx;        // fused FP32 path: hardware-reciprocal ratios (approx_div form)
+    int zdepth;        // fused path: planes per CTA z chunk (0 = the whole column)
 };
 
 // Ensemble (batched 2D instances): per-instance descriptor with the element

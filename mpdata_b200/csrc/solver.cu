@@ -159,6 +159,24 @@ using mpd::Solver;
 
 namespace {
 
+// Default z-chunk depth of the fused kernels: enough CTAs for about four
+// waves of two CTAs per SM, never chunks thinner than 8 planes.
+int default_zdepth(const mpd::Solver* h)
+{
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    const int ow = h->opts.limiter ? 1 : 0;
+    const long long bx = (h->d.nx - 2 + 32 - 2 * ow - 1) / (32 - 2 * ow);
+    const long long by = (h->d.ny - 2 + 16 - 2 * ow - 1) / (16 - 2 * ow);
+    const long long want = 4LL * 2 * sms;
+    const int interior = h->d.ns - 2;
+    long long chunks = (want + bx * by - 1) / (bx * by);
+    if (chunks < 1) chunks = 1;
+    int depth = (int)((interior + chunks - 1) / chunks);
+    if (depth < 8) depth = 8;
+    return depth >= interior ? 0 : depth;
+}
+
 int check_dims(int nx, int ny, int ns)
 {
     if (nx < 3 || ny < 3 || ns < 3)
@@ -303,6 +321,7 @@ template <typename T> int step_impl(Solver* h, int nsteps)
             a.wide = h->opts.precision_form;
             a.write_faces = o < P - 1;
             a.approx = h->opts.approx_div;
+            a.zdepth = h->zdepth;
             {
                 PassTimer timer(h, a.write_faces ? 1 : 2);
                 if (fused) op.pass_fused(d, a, h->stream);
@@ -444,6 +463,7 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     CUDA_TRY(cudaGetDevice(&h->device));
     CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
+    h->zdepth = default_zdepth(h.get());
     if (int rc = alloc_solver(h.get())) {
         free_solver(h.get());
         return rc == MPDATA_ERR_CUDA ? fail(MPDATA_ERR_NOMEM, "device allocation failed: %s",
@@ -694,6 +714,65 @@ int mpdata_launches_per_step(mpdata_handle h)
 {
     if (!h) return mpd::fail(MPDATA_ERR_ARG, "null handle");
     return mpd::launches(reinterpret_cast<Solver*>(h));
+}
+
+int mpdata_set_march_depth(mpdata_handle hh, int depth)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h || depth < 0) return mpd::fail(MPDATA_ERR_ARG, "bad arguments");
+    h->zdepth = depth >= h->d.ns - 2 ? 0 : depth;
+    return 0;
+}
+
+int mpdata_march_depth(mpdata_handle hh)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h) return mpd::fail(MPDATA_ERR_ARG, "null handle");
+    return h->zdepth;
+}
+
+int mpdata_autotune(mpdata_handle hh, int trial_steps, int* depth_out, double* ms_out)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h || trial_steps < 1) return mpd::fail(MPDATA_ERR_ARG, "bad arguments");
+    if (!h->have_field || !h->have_faces) return mpd::fail(MPDATA_ERR_STATE, "field and faces first");
+    if (int rc = ensure_device(h)) return rc;
+    const size_t fb = field_bytes(h);
+    void* saved = nullptr;
+    CUDA_TRY(cudaMalloc(&saved, fb));
+    CUDA_TRY(cudaMemcpyAsync(saved, h->c[h->cur], fb, cudaMemcpyDeviceToDevice, h->stream));
+    const int interior = h->d.ns - 2;
+    const int cand[] = {0, 128, 64, 32, 16, 8};
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    int best = h->zdepth;
+    double best_ms = 1e300;
+    for (int c : cand) {
+        if (c != 0 && c >= interior) continue;
+        h->zdepth = c;
+        if (int rc = mpd::step(h, 1)) { cudaFree(saved); return rc; }
+        CUDA_TRY(cudaEventRecord(e0, h->stream));
+        if (int rc = mpd::step(h, trial_steps)) { cudaFree(saved); return rc; }
+        CUDA_TRY(cudaEventRecord(e1, h->stream));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best_ms) { best_ms = ms; best = c; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->zdepth = best;
+    // put the field back as it was (all three levels, as set_field does)
+    for (int b = 0; b < 3; b++)
+        CUDA_TRY(cudaMemcpyAsync(h->c[b], saved, fb, cudaMemcpyDeviceToDevice, h->stream));
+    h->cur = 0;
+    h->prev = 0;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    cudaFree(saved);
+    if (depth_out) *depth_out = best;
+    if (ms_out) *ms_out = best_ms / trial_steps;
+    return mpd::check_device_error(h);
 }
 
 int mpdata_enable_pass_timing(mpdata_handle hh, int on)

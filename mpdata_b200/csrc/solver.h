@@ -37,6 +37,7 @@ struct Solver {
     CUtensorMap tm_c[3];
     CUtensorMap tm_f[3][3];
     bool have_field = false, have_faces = false;
+    int zdepth = 0;  // fused kernels: planes per z chunk (set by the default heuristic / autotuner)
     // Optional per-pass event timing: pending event pairs per pass class.
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[3];

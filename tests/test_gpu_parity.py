@@ -105,6 +105,49 @@ def test_handle_strict_bit_exact(m, kernel, dtype, shape, order, opt):
     assert np.array_equal(got, ref), np.abs(got - ref).max()
 
 
+@pytest.mark.parametrize("depth", [1, 2, 5, 13, 0])
+@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("limiter", [0, 1])
+def test_z_chunked_march_strict_bit_exact(m, depth, order, limiter):
+    """Chunking the z march (any depth, chunk edges anywhere) changes nothing."""
+    import oracle
+    nx, ny, ns = 37, 21, 30
+    case = workloads.random_case(nx, ny, ns, seed=depth + 7 * order)
+    U, V, W = _faces(case, np.float32)
+    c = case["c0"].astype(np.float32)
+    ref = c
+    for _ in range(2):
+        ref = oracle.step_faces(U, V, W, ref, order, limiter=limiter)
+    with m.Solver(nx, ny, ns, order=order, strict=True, limiter=bool(limiter)) as s:
+        s.set_march_depth(depth)
+        s.set_faces(U, V, W)
+        s.set_field(c)
+        s.step(2)
+        assert np.array_equal(s.get_field(), ref)
+
+
+def test_autotune_keeps_field_and_results():
+    import oracle
+    nx, ny, ns = 66, 34, 40
+    case = workloads.random_case(nx, ny, ns, seed=21)
+    U, V, W = _faces(case, np.float32)
+    c = case["c0"].astype(np.float32)
+    ref = oracle.step_faces(U, V, W, c, 3, limiter=1)
+    with m_solver(nx, ny, ns) as s:
+        s.set_faces(U, V, W)
+        s.set_field(c)
+        depth, ms = s.autotune(trial_steps=2)
+        assert ms > 0 and depth in (0, 128, 64, 32, 16, 8)
+        assert np.array_equal(s.get_field(), c)
+        s.step(1)
+        assert np.array_equal(s.get_field(), ref)
+
+
+def m_solver(nx, ny, ns):
+    import mpdata_b200
+    return mpdata_b200.Solver(nx, ny, ns, order=3, strict=True, limiter=True)
+
+
 @pytest.mark.parametrize("kernel", [0, 1], ids=["fused", "unfused"])
 @pytest.mark.parametrize("order", [2, 3])
 def test_precision_form_strict_bit_exact(m, kernel, order):
