@@ -75,7 +75,7 @@ int smolar_f64(int nx, int ny, int ns, double* dx, double* dy, double* ds,
  * state between calls and is released by msmolar_free().  Every step
  * exchanges block halos deep enough for all `order` passes, so the result
  * equals smolar() on the whole grid (the reference's intent; its own 1-cell
- * halo does not achieve that).  The caller's *c0/*c1 pointers are exchanged
+ * halo does not achieve that).  The caller's *c0 and *c1 pointers are exchanged
  * the way smolar() exchanges them, and the caller's arrays are brought up to
  * date only by msmolar_gather().  flow_type and mode are ignored.
  *
@@ -102,8 +102,12 @@ const char* mpdata_last_error(void);
 
 struct mpdata_options;
 /* Options used by smolar(), smolar_f64() and msmolar() on the calling thread
- * (NULL restores the defaults: reference behaviour, fused kernels).  No
- * reference counterpart: the reference has no run-time options. */
+ * (NULL restores the defaults: reference behaviour, fused kernels).  Each
+ * thread starts from the environment variable MPDATA_B200_OPTIONS, a
+ * comma-separated list of limiter, precision_form, strict, unfused, vv_fix,
+ * div_off, approx_div, check_courant, so programs written against the
+ * reference API can select options without code changes.  No reference
+ * counterpart: the reference has no run-time options. */
 int mpdata_set_default_options(const struct mpdata_options* opts);
 
 /* ---- 2. Device-resident handle API ---------------------------------------- */

@@ -18,8 +18,10 @@
 // tests compare a buffer with itself, tests/init.c:114-115).
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "mpdata_b200.h"
@@ -48,7 +50,40 @@ struct HostCache {
     }
 };
 thread_local HostCache g_cache;
-thread_local mpdata_options g_opts{};  // options of smolar()/msmolar() on this thread
+// Options of smolar()/msmolar() on this thread.  Start from the environment
+// variable MPDATA_B200_OPTIONS (comma-separated: limiter, precision_form,
+// strict, unfused, vv_fix, div_off, approx_div, check_courant), so programs
+// written against the reference API, which has no options call, can still
+// select them.
+mpdata_options env_options()
+{
+    mpdata_options o;
+    memset(&o, 0, sizeof o);
+    const char* s = getenv("MPDATA_B200_OPTIONS");
+    if (!s) return o;
+    std::string v(s);
+    auto has = [&](const char* w) {
+        size_t p = 0, n = strlen(w);
+        while ((p = v.find(w, p)) != std::string::npos) {
+            bool start = p == 0 || v[p - 1] == ',';
+            bool end = p + n == v.size() || v[p + n] == ',';
+            if (start && end) return true;
+            p += n;
+        }
+        return false;
+    };
+    o.limiter = has("limiter");
+    o.precision_form = has("precision_form");
+    o.strict = has("strict");
+    o.kernel = has("unfused") ? 1 : 0;
+    o.vv_fix = has("vv_fix");
+    o.div_mode = has("div_off") ? MPDATA_DIV_OFF : MPDATA_DIV_REFERENCE;
+    o.approx_div = has("approx_div");
+    o.check_courant = has("check_courant");
+    return o;
+}
+
+thread_local mpdata_options g_opts = env_options();
 
 bool same_options(const mpdata_options& a, const mpdata_options& b)
 {

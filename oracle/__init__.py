@@ -39,6 +39,11 @@ def build(reference: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if reference and os.path.isdir(os.path.join(REFERENCE_SRC, "core", "src")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_SRC}"], check=True)
+        # the reference's ring drivers, also linked against the GPU library once it is built
+        lib = os.path.join(os.path.dirname(HERE), "mpdata_b200", "libmpdata_b200.so")
+        if os.path.exists(lib):
+            subprocess.run(["make", "-s", "-C", HERE, "drivers", f"REF={REFERENCE_SRC}"],
+                           check=True)
 
 
 _libs: dict[str, C.CDLL] = {}
