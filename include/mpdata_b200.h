@@ -104,8 +104,8 @@ struct mpdata_options;
 /* Options used by smolar(), smolar_f64() and msmolar() on the calling thread
  * (NULL restores the defaults: reference behaviour, fused kernels).  Each
  * thread starts from the environment variable MPDATA_B200_OPTIONS, a
- * comma-separated list of limiter, precision_form, strict, unfused, vv_fix,
- * div_off, approx_div, check_courant, so programs written against the
+ * comma-separated list of limiter, precision_form, strict, unfused, single,
+ * vv_fix, div_off, approx_div, check_courant, so programs written against the
  * reference API can select options without code changes.  No reference
  * counterpart: the reference has no run-time options. */
 int mpdata_set_default_options(const struct mpdata_options* opts);
@@ -133,8 +133,10 @@ typedef struct mpdata_options {
                            unwritten (vv.c:81-82) instead of its buffer rule */
     int strict;         /* 1: no FMA contraction; bit-identical to a strict-IEEE
                            CPU build of the reference arithmetic */
-    int kernel;         /* 0: fused per-pass kernels (default); 1: one kernel per
-                           reference function (slower; cross-check path) */
+    int kernel;         /* 0: fused per-pass kernels (default; two cells per thread
+                           for F32 without strict or precision_form); 1: one kernel
+                           per reference function (slower; cross-check path);
+                           2: fused, one cell per thread */
     int check_courant;  /* 1: reject advective faces with |Courant| > 1 */
     int approx_div;     /* 1 (F32, fused kernels, not strict): the ratios of the
                            antidiffusive velocity and of the limiter use the

@@ -241,7 +241,9 @@ class SolverOptions:
     div_mode: int = DIV_REFERENCE
     vv_fix: bool = False
     strict: bool = False
-    kernel: int = 0  # 0 fused per-pass kernels, 1 one kernel per reference routine
+    # 0 fused per-pass kernels (two cells per thread where the arithmetic allows),
+    # 1 one kernel per reference routine, 2 fused with one cell per thread
+    kernel: int = 0
     check_courant: bool = False
     approx_div: bool = False
 

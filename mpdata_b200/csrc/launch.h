@@ -26,9 +26,20 @@ struct PassMaps {
 // above; y: two halo rows below, 16 + 1 above).
 constexpr int kBoxX = 40, kBoxY = 19;
 
+// Two-cells-per-thread fast pass (kernels_pair.cuh): CTAs of 32 x kPairCY
+// cells staged as 40 x (kPairCY + 2) boxes (x: two columns below plus up to
+// two of alignment slack, y: one row below and one above).  16 rows: two
+// CTAs of 256 threads per SM (measured faster than one CTA of 32 rows).
+#ifndef MPD_PAIR_CY
+#define MPD_PAIR_CY 16
+#endif
+constexpr int kPairCY = MPD_PAIR_CY;
+constexpr int kPairBoxX = 40, kPairBoxY = kPairCY + 2;
+
 // Per-pass description for the corrective-pass launchers.
 template <typename T> struct PassArgs {
     PassMaps maps;     // fused path: descriptors of c, cn, Uo, Vo, Wo
+    PassMaps maps2;    // the same arrays with the two-cell pass's boxes
     int* err;          // device error word (bounded-wait timeouts); may be null
     const T* c;        // this pass's input field (level o)
     const T* cn;       // the step's input field (limiter bounds); may be null without limiter
@@ -117,7 +128,11 @@ template <typename T> struct AdjPassArgs {
     template <typename T>                                                                  \
     int launch_pass_fused(const Dims& d, const PassArgs<T>& a, cudaStream_t s);
 
-namespace fast { MPD_DECLARE_LAUNCHERS }
+namespace fast {
+MPD_DECLARE_LAUNCHERS
+/* Corrective pass, two cells per thread (FP32, regrouped arithmetic: fast mode only). */
+int launch_pass_pair(const Dims& d, const PassArgs<float>& a, cudaStream_t s);
+}
 namespace strict { MPD_DECLARE_LAUNCHERS }
 
 // Mode-independent utility kernels (reductions, fills), in solver.cu.

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 
 #include "launch.h"
 #include "mpdata_b200.h"
@@ -160,15 +161,26 @@ using mpd::Solver;
 namespace {
 
 // Default z-chunk depth of the fused kernels: enough CTAs for about four
-// waves of two CTAs per SM, never chunks thinner than 8 planes.
+// waves (two CTAs per SM for the one-cell pass, one for the two-cell pass),
+// never chunks thinner than 8 planes.
 int default_zdepth(const mpd::Solver* h)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-    const int ow = h->opts.limiter ? 1 : 0;
-    const long long bx = (h->d.nx - 2 + 32 - 2 * ow - 1) / (32 - 2 * ow);
-    const long long by = (h->d.ny - 2 + 16 - 2 * ow - 1) / (16 - 2 * ow);
-    const long long want = 4LL * 2 * sms;
+    const bool lim = h->opts.limiter != 0;
+    int sx, sy, per_sm;
+    if (h->pair) {
+        sx = lim ? 28 : 30;
+        sy = lim ? mpd::kPairCY - 3 : mpd::kPairCY - 1;
+        per_sm = mpd::kPairCY >= 32 ? 1 : 2;
+    } else {
+        sx = lim ? 30 : 32;
+        sy = lim ? 14 : 16;
+        per_sm = 2;
+    }
+    const long long bx = (h->d.nx - 2 + sx - 1) / sx;
+    const long long by = (h->d.ny - 2 + sy - 1) / sy;
+    const long long want = 4LL * per_sm * sms;
     const int interior = h->d.ns - 2;
     long long chunks = (want + bx * by - 1) / (bx * by);
     if (chunks < 1) chunks = 1;
@@ -288,7 +300,7 @@ template <typename T> int step_impl(Solver* h, int nsteps)
     ModeOps<T> op = ops<T>(h);
     const Dims& d = h->d;
     const int P = h->order;
-    const bool fused = h->opts.kernel == 0;
+    const bool fused = h->opts.kernel != 1;
     for (int s = 0; s < nsteps; s++) {
         const int b0 = h->cur, b1 = (b0 + 1) % 3, b2 = (b0 + 2) % 3;
         // pass 0: donor cell with the advective faces
@@ -303,6 +315,8 @@ template <typename T> int step_impl(Solver* h, int nsteps)
             const int ws = 1 + ((o - 1) & 1);
             mpd::PassArgs<T> a;
             a.maps = {&h->tm_c[in], &h->tm_c[b0], &h->tm_f[rs][0], &h->tm_f[rs][1], &h->tm_f[rs][2]};
+            a.maps2 = {&h->tm2_c[in], &h->tm2_c[b0], &h->tm2_f[rs][0], &h->tm2_f[rs][1],
+                       &h->tm2_f[rs][2]};
             a.err = h->dev_err;
             a.c = Cb<T>(h, in);
             a.cn = Cb<T>(h, b0);
@@ -324,8 +338,17 @@ template <typename T> int step_impl(Solver* h, int nsteps)
             a.zdepth = h->zdepth;
             {
                 PassTimer timer(h, a.write_faces ? 1 : 2);
-                if (fused) op.pass_fused(d, a, h->stream);
-                else op.pass_unfused(d, a, (T*)h->bup, (T*)h->bdn, h->stream);
+                bool done = false;
+                if constexpr (std::is_same<T, float>::value) {
+                    if (h->pair) {
+                        mpd::fast::launch_pass_pair(d, a, h->stream);
+                        done = true;
+                    }
+                }
+                if (!done) {
+                    if (fused) op.pass_fused(d, a, h->stream);
+                    else op.pass_unfused(d, a, (T*)h->bup, (T*)h->bdn, h->stream);
+                }
             }
             int t = in; in = out; out = t;
         }
@@ -340,7 +363,7 @@ template <typename T> int launches_per_step(const Solver* h)
 {
     int n = 1;  // donor pass
     for (int o = 1; o < h->order; o++) {
-        if (h->opts.kernel == 0) n += 1;
+        if (h->opts.kernel != 1) n += 1;
         else n += h->opts.limiter ? 4 : 2;
     }
     return n;
@@ -367,13 +390,14 @@ EncodeTiledFn encode_fn()
 }
 
 // Descriptor of one full-grid array for the fused kernels' per-plane boxes.
-int make_map(const Solver* h, void* ptr, CUtensorMap* map)
+int make_map(const Solver* h, void* ptr, CUtensorMap* map, int box_x = mpd::kBoxX,
+             int box_y = mpd::kBoxY)
 {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return mpd::fail(MPDATA_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     cuuint64_t dims[3] = {(cuuint64_t)h->d.nx, (cuuint64_t)h->d.ny, (cuuint64_t)h->d.ns};
     cuuint64_t strides[2] = {(cuuint64_t)(h->d.px * h->esz), (cuuint64_t)(h->d.pp * h->esz)};
-    cuuint32_t box[3] = {(cuuint32_t)mpd::kBoxX, (cuuint32_t)mpd::kBoxY, 1};
+    cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
     cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = enc(map, h->dtype == MPDATA_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
@@ -392,14 +416,23 @@ int alloc_solver(Solver* h)
         for (int a = 0; a < 3; a++) CUDA_TRY(cudaMalloc(&h->faces[s][a], fb));
     CUDA_TRY(cudaMalloc(&h->dev_err, sizeof(int)));
     CUDA_TRY(cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream));
-    if (h->opts.kernel == 0) {
+    if (h->opts.kernel != 1) {
         for (int b = 0; b < 3; b++)
             if (int rc = make_map(h, h->c[b], &h->tm_c[b])) return rc;
         for (int s = 0; s < 3; s++)
             for (int a = 0; a < 3; a++)
                 if (int rc = make_map(h, h->faces[s][a], &h->tm_f[s][a])) return rc;
     }
-    if (h->opts.kernel != 0 && h->opts.limiter) {
+    if (h->pair) {
+        for (int b = 0; b < 3; b++)
+            if (int rc = make_map(h, h->c[b], &h->tm2_c[b], mpd::kPairBoxX, mpd::kPairBoxY)) return rc;
+        for (int s = 0; s < 3; s++)
+            for (int a = 0; a < 3; a++)
+                if (int rc = make_map(h, h->faces[s][a], &h->tm2_f[s][a], mpd::kPairBoxX,
+                                      mpd::kPairBoxY))
+                    return rc;
+    }
+    if (h->opts.kernel == 1 && h->opts.limiter) {
         CUDA_TRY(cudaMalloc(&h->bup, fb));
         CUDA_TRY(cudaMalloc(&h->bdn, fb));
     }
@@ -447,8 +480,8 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     if (opts) o = *opts;
     if (o.precision_form && dtype != MPDATA_F32)
         return fail(MPDATA_ERR_ARG, "precision_form applies to float storage only");
-    if (o.kernel < 0 || o.kernel > 1) return fail(MPDATA_ERR_ARG, "bad kernel option %d", o.kernel);
-    if (o.approx_div && (dtype != MPDATA_F32 || o.strict || o.kernel != 0))
+    if (o.kernel < 0 || o.kernel > 2) return fail(MPDATA_ERR_ARG, "bad kernel option %d", o.kernel);
+    if (o.approx_div && (dtype != MPDATA_F32 || o.strict || o.kernel == 1))
         return fail(MPDATA_ERR_ARG, "approx_div needs float storage, fused kernels and no strict mode");
     std::unique_ptr<Solver> h(new Solver());
     h->dtype = dtype;
@@ -463,6 +496,11 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     CUDA_TRY(cudaGetDevice(&h->device));
     CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
+    // The two-cell pass: FP32, fast arithmetic, FP32 limiter ratios, fused kernels by
+    // default.  With the limiter and IEEE division the one-cell pass is faster on B200
+    // (the division slow paths spill the two-cell kernel's registers), so it keeps it.
+    h->pair = dtype == MPDATA_F32 && !o.strict && !o.precision_form && o.kernel == 0 &&
+              (o.approx_div || !o.limiter);
     h->zdepth = default_zdepth(h.get());
     if (int rc = alloc_solver(h.get())) {
         free_solver(h.get());
@@ -742,7 +780,7 @@ int mpdata_autotune(mpdata_handle hh, int trial_steps, int* depth_out, double* m
     CUDA_TRY(cudaMalloc(&saved, fb));
     CUDA_TRY(cudaMemcpyAsync(saved, h->c[h->cur], fb, cudaMemcpyDeviceToDevice, h->stream));
     const int interior = h->d.ns - 2;
-    const int cand[] = {0, 128, 64, 32, 16, 8};
+    const int cand[] = {0, 128, 96, 64, 48, 32, 24, 16, 8};
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));

@@ -36,6 +36,10 @@ struct Solver {
     // TMA descriptors of the three field levels and the nine face arrays.
     CUtensorMap tm_c[3];
     CUtensorMap tm_f[3][3];
+    // Two-cells-per-thread pass (FP32 fast arithmetic): its own descriptors (larger boxes).
+    bool pair = false;
+    CUtensorMap tm2_c[3];
+    CUtensorMap tm2_f[3][3];
     bool have_field = false, have_faces = false;
     int zdepth = 0;  // fused kernels: planes per z chunk (set by the default heuristic / autotuner)
     // Optional per-pass event timing: pending event pairs per pass class.
