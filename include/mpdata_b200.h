@@ -105,7 +105,7 @@ struct mpdata_options;
  * (NULL restores the defaults: reference behaviour, fused kernels).  Each
  * thread starts from the environment variable MPDATA_B200_OPTIONS, a
  * comma-separated list of limiter, precision_form, strict, unfused, single,
- * vv_fix, div_off, approx_div, check_courant, so programs written against the
+ * pair, vv_fix, div_off, approx_div, check_courant, so programs written against the
  * reference API can select options without code changes.  No reference
  * counterpart: the reference has no run-time options. */
 int mpdata_set_default_options(const struct mpdata_options* opts);
@@ -133,10 +133,11 @@ typedef struct mpdata_options {
                            unwritten (vv.c:81-82) instead of its buffer rule */
     int strict;         /* 1: no FMA contraction; bit-identical to a strict-IEEE
                            CPU build of the reference arithmetic */
-    int kernel;         /* 0: fused per-pass kernels (default; two cells per thread
-                           for F32 without strict or precision_form); 1: one kernel
-                           per reference function (slower; cross-check path);
-                           2: fused, one cell per thread */
+    int kernel;         /* 0: fused per-pass kernels, the faster of the two forms
+                           below for the options (default); 1: one kernel per
+                           reference function (slower; cross-check path);
+                           2: fused, one cell per thread; 3: fused, two cells per
+                           thread (F32 without strict or precision_form) */
     int check_courant;  /* 1: reject advective faces with |Courant| > 1 */
     int approx_div;     /* 1 (F32, fused kernels, not strict): the ratios of the
                            antidiffusive velocity and of the limiter use the

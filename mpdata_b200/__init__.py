@@ -241,8 +241,9 @@ class SolverOptions:
     div_mode: int = DIV_REFERENCE
     vv_fix: bool = False
     strict: bool = False
-    # 0 fused per-pass kernels (two cells per thread where the arithmetic allows),
-    # 1 one kernel per reference routine, 2 fused with one cell per thread
+    # 0 fused per-pass kernels (the faster form for the options), 1 one kernel per
+    # reference routine, 2 fused with one cell per thread, 3 fused with two cells
+    # per thread (float32 without strict / precision_form)
     kernel: int = 0
     check_courant: bool = False
     approx_div: bool = False

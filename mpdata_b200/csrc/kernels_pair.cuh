@@ -50,10 +50,13 @@ constexpr int NSTAGE = 4;
 constexpr int WX = 36, WY = CY + 1, WPL = WX * WY;  // work planes: x [-2, 33], y [-1, CY-1]
 
 __host__ __device__ constexpr int stage_bytes() { return (SBX * SBY * 4 + 127) / 128 * 128; }
-template <bool LIM> __host__ __device__ constexpr int n_work() { return LIM ? 10 : 2; }
+// staged arrays: c, Uo, Vo, Wo (+ c^n with the limiter)
+template <bool LIM> __host__ __device__ constexpr int n_arrays() { return LIM ? 5 : 4; }
+template <bool LIM> __host__ __device__ constexpr int n_work() { return LIM ? 12 : 2; }
 template <bool LIM> __host__ __device__ constexpr size_t smem_bytes()
 {
-    return (size_t)NSTAGE * 4 * stage_bytes() + (size_t)n_work<LIM>() * WPL * 4 + NSTAGE * 8;
+    return (size_t)NSTAGE * n_arrays<LIM>() * stage_bytes() + (size_t)n_work<LIM>() * WPL * 4 +
+           NSTAGE * 8;
 }
 // Tile strides: cells of a CTA that are updated (x: 3..30 / 1..30, y: 2..CY-2 / 1..CY-1).
 template <bool LIM> __host__ __device__ constexpr int stride_x() { return LIM ? CX - 4 : CX - 2; }
@@ -307,54 +310,72 @@ __device__ __forceinline__ float limit(float a, float bu_lo, float bd_lo, float 
 
 }  // namespace pair
 
-template <bool LIM, bool AP, bool BORDER>
-__device__ __forceinline__ void pair_march(const Dims& d, const PassArgs<float>& a,
-                                           const CUtensorMap* map_c, const CUtensorMap* map_uo,
-                                           const CUtensorMap* map_vo, const CUtensorMap* map_wo,
-                                           unsigned char* smem, int i0, int j0)
+// Per-thread placement shared by both marches.
+struct PairSetup {
+    int gx0, gy0;       // box origin of the staged planes (x 16-byte aligned)
+    int o, w;           // cell A in a staged plane / a work plane (both even: 8-byte pairs)
+    int xA, iA, j;      // local x of A, global i of A, global j
+    pair::PairGeo g;
+    bool ownA, ownB;    // cells this CTA updates
+    bool wxA, wxB, wyA, wyB;  // x / y faces this CTA writes (incl. the low domain faces)
+    long long col;      // element offset of (iA, j, 0)
+};
+
+template <bool LIM, bool BORDER>
+__device__ __forceinline__ PairSetup pair_setup(const Dims& d, const PassArgs<float>& a, int i0, int j0)
 {
     using namespace pair;
-    constexpr int SB = stage_bytes();
-    constexpr int Y = SBX;
-    float* work = reinterpret_cast<float*>(smem + (size_t)NSTAGE * 4 * SB);
-    // limiter: fluxes of the raw high faces, bound extrema, ratios, donor fluxes (two slots)
-    float* sFX = work;
-    float* sFY = sFX + WPL;
-    float* sMX = sFY + WPL;
-    float* sMN = sMX + WPL;
-    float* sBU = sMN + WPL;
-    float* sBD = sBU + WPL;
-    float* sDX = LIM ? sBD + WPL : work;          // donor x fluxes (LIM: slots at +0 / +WPL)
-    float* sDY = LIM ? sDX + 2 * WPL : work + WPL;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(work + n_work<LIM>() * WPL);
-
-    const int ny = d.ny, ns = d.ns;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int gx0 = (i0 - 2) & ~3, gy0 = j0 - 1, rx = (i0 - 2) - gx0;
-    const int o = (ty + 1) * Y + 2 * tx + 2 + rx;  // cell A in a staged plane (even: 8-byte pairs)
-    const int w = (ty + 1) * WX + 2 * tx + 2;      // cell A in a work plane (even)
-    const int xA = 2 * tx;
-    const int iA = i0 + xA, j = j0 + ty;
-    const PairGeo g = pair_geo(d, iA, j, a.vv_fix);
-    // cells this CTA updates (and whose faces it writes)
+    PairSetup p;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    p.gx0 = (i0 - 2) & ~3;
+    p.gy0 = j0 - 1;
+    const int rx = (i0 - 2) - p.gx0;
+    p.o = (ty + 1) * SBX + 2 * tx + 2 + rx;
+    p.w = (ty + 1) * WX + 2 * tx + 2;
+    p.xA = 2 * tx;
+    p.iA = i0 + p.xA;
+    p.j = j0 + ty;
+    p.g = pair_geo(d, p.iA, p.j, a.vv_fix);
     const int ox0 = LIM ? 3 : 1, ox1 = CX - 2, oy0 = LIM ? 2 : 1, oy1 = LIM ? CY - 2 : CY - 1;
     const bool own_y = ty >= oy0 && ty <= oy1;
-    const bool ownA = own_y && xA >= ox0 && xA <= ox1 && (!BORDER || g.cx);
-    const bool ownB = own_y && xA + 1 >= ox0 && xA + 1 <= ox1 && (!BORDER || g.cy);
+    const bool inA = p.xA >= ox0 && p.xA <= ox1, inB = p.xA + 1 >= ox0 && p.xA + 1 <= ox1;
+    p.ownA = own_y && inA && (!BORDER || p.g.cx);
+    p.ownB = own_y && inB && (!BORDER || p.g.cy);
     // faces on the low domain boundary are written by the CTA holding the shell cell
-    const bool wxA = own_y && ((xA >= ox0 && xA <= ox1) || iA == 0) && g.ux;
-    const bool wxB = own_y && ((xA + 1 >= ox0 && xA + 1 <= ox1) || iA + 1 == 0) && g.uy;
-    const bool wy_row = own_y || j == 0;
-    const bool wyA = wy_row && xA >= ox0 && xA <= ox1 && g.vx;
-    const bool wyB = wy_row && xA + 1 >= ox0 && xA + 1 <= ox1 && g.vy;
-    // The step input c^n: 64-bit loads of the pair (rows inside the grid,
-    // columns inside the pitch).  The ring cells on the high sides (x = 31,
-    // y = CY-1) bound over a neighbour outside the CTA, whose c^n the edge
-    // threads read as well (x + 2 / the row above).
-    const bool cn_ok = LIM && j >= 0 && j < ny && iA >= 0 && iA < d.px;
-    const bool edge_x = LIM && tx == TX - 1, edge_y = LIM && ty == CY - 1;
-    const bool cnR_ok = edge_x && j >= 0 && j < ny && iA + 2 < d.px;
-    const bool cnU_ok = edge_y && j + 1 >= 0 && j + 1 < ny && iA >= 0 && iA < d.px;
+    p.wxA = own_y && (inA || p.iA == 0) && p.g.ux;
+    p.wxB = own_y && (inB || p.iA + 1 == 0) && p.g.uy;
+    const bool wy_row = own_y || p.j == 0;
+    p.wyA = wy_row && inA && p.g.vx;
+    p.wyB = wy_row && inB && p.g.vy;
+    p.col = (long long)p.j * d.px + p.iA;
+    return p;
+}
+
+__device__ __forceinline__ void store_pair(float* out, float2 v, bool a, bool b)
+{
+    if (a && b) pair::st2(out, v);
+    else if (a) out[0] = v.x;
+    else if (b) out[1] = v.y;
+}
+
+// ---- without the limiter: faces of plane k -> sync -> update of plane k ----
+template <bool AP, bool BORDER>
+__device__ __forceinline__ void pair_march_plain(const Dims& d, const PassArgs<float>& a,
+                                                 const CUtensorMap* map_c, const CUtensorMap* map_uo,
+                                                 const CUtensorMap* map_vo, const CUtensorMap* map_wo,
+                                                 unsigned char* smem, int i0, int j0)
+{
+    using namespace pair;
+    constexpr int NARR = n_arrays<false>();
+    constexpr int SB = stage_bytes();
+    float* work = reinterpret_cast<float*>(smem + (size_t)NSTAGE * NARR * SB);
+    float* sDX = work;        // donor fluxes through the x faces of plane k (A|B, B|x+2)
+    float* sDY = work + WPL;  // through the y faces
+    uint64_t* bars = reinterpret_cast<uint64_t*>(work + n_work<false>() * WPL);
+    const PairSetup p = pair_setup<false, BORDER>(d, a, i0, j0);
+    const int ns = d.ns;
+    const int tid = threadIdx.y * TX + threadIdx.x;
+    const long long pp = d.pp;
 
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) tma::mbar_init(&bars[s], 1);
@@ -365,43 +386,176 @@ __device__ __forceinline__ void pair_march(const Dims& d, const PassArgs<float>&
         tma::prefetch_map(map_wo);
     }
     __syncthreads();
-
     auto slot = [&](int s, int arr) -> const float* {
-        return reinterpret_cast<const float*>(smem + (size_t)(s * 4 + arr) * SB);
+        return reinterpret_cast<const float*>(smem + (size_t)(s * NARR + arr) * SB);
     };
-    auto issue = [&](int p) {
-        const int s = p & (NSTAGE - 1);
+    auto issue = [&](int pl) {
+        const int s = pl & (NSTAGE - 1);
         uint64_t* bar = &bars[s];
         tma::fence_proxy_async_shared();
-        tma::mbar_arrive_expect_tx(bar, (uint32_t)(4 * SBX * SBY * sizeof(float)));
-        tma::load_3d(const_cast<float*>(slot(s, 0)), map_c, gx0, gy0, p, bar);
-        tma::load_3d(const_cast<float*>(slot(s, 1)), map_uo, gx0, gy0, p, bar);
-        tma::load_3d(const_cast<float*>(slot(s, 2)), map_vo, gx0, gy0, p, bar);
-        tma::load_3d(const_cast<float*>(slot(s, 3)), map_wo, gx0, gy0, p, bar);
-    };
-    // global element offsets: the pair's column (plane 0) and one plane
-    const long long col = (long long)j * d.px + iA, pp = d.pp;
-    const float* cn_col = a.cn + col;
-    auto ldcn = [&](int k, long long kp) -> float2 {
-        if (!cn_ok || k > ns - 1) return bc(0.f);
-        return *reinterpret_cast<const float2*>(cn_col + kp);
-    };
-    auto ldcnR = [&](int k, long long kp) -> float {
-        if (!cnR_ok || k > ns - 1) return 0.f;
-        return cn_col[kp + 2];
-    };
-    auto ldcnU = [&](int k, long long kp) -> float2 {
-        if (!cnU_ok || k > ns - 1) return bc(0.f);
-        return *reinterpret_cast<const float2*>(cn_col + kp + d.px);
+        tma::mbar_arrive_expect_tx(bar, (uint32_t)(NARR * SBX * SBY * sizeof(float)));
+        tma::load_3d(const_cast<float*>(slot(s, 0)), map_c, p.gx0, p.gy0, pl, bar);
+        tma::load_3d(const_cast<float*>(slot(s, 1)), map_uo, p.gx0, p.gy0, pl, bar);
+        tma::load_3d(const_cast<float*>(slot(s, 2)), map_vo, p.gx0, p.gy0, pl, bar);
+        tma::load_3d(const_cast<float*>(slot(s, 3)), map_wo, p.gx0, p.gy0, pl, bar);
     };
 
-    // z chunk (see k_pass_tma): warm-up planes so the first updated plane sees
-    // exactly what an unchunked march would form.
+    // z chunk (see k_pass_tma): two warm-up planes, the first for the z face below
     const int depth = a.zdepth > 0 ? a.zdepth : ns - 2;
     const int z0 = 1 + (int)blockIdx.z * depth;
     const int z1 = min(ns - 1, z0 + depth);
-    const int kstart = max(0, z0 - (LIM ? 3 : 2));
-    const int last = LIM ? z1 : z1 - 1;
+    const int kstart = max(0, z0 - 2);
+    const int last = z1 - 1;
+    const int issue_max = min(ns - 1, last + 1);
+
+    bool ok = true;
+    int confirmed = kstart;
+    if (tid == 0) {
+        issue(kstart);
+        issue(kstart + 1);
+    }
+    ok = tma::mbar_wait(&bars[kstart & (NSTAGE - 1)], 0);
+    if (tid == 0 && ok) confirmed = kstart + 1;
+    float2 cq1 = bc(0.f), cq2 = ok ? ld2(slot(kstart & (NSTAGE - 1), 0) + p.o) : bc(0.f), cq3 = bc(0.f);
+    float2 dz_prev = bc(0.f);  // donor flux through the z face below plane k
+
+    auto plane = [&](auto Sc, const int k) {
+        constexpr int S = decltype(Sc)::value;
+        constexpr int SM1 = (S + NSTAGE - 1) % NSTAGE, SP1 = (S + 1) % NSTAGE;
+        __syncthreads();  // every read of the slot plane k+2 reuses is done
+        if (tid == 0 && k + 2 <= issue_max) issue(k + 2);
+        if (k + 1 <= ns - 1) {
+            if (ok) ok = tma::mbar_wait(&bars[SP1], ((k + 1 - kstart) / NSTAGE) & 1);
+            if (tid == 0 && ok) confirmed = k + 2;
+            cq3 = ld2(slot(SP1, 0) + p.o);
+        }
+        const bool kin = k >= 1 && k <= ns - 2;
+        float2 ru = bc(0.f), rv = bc(0.f), rw = bc(0.f), cU;
+        float c2;
+        {
+            const PairNb nb = gather(slot(SM1, 0), slot(S, 0), slot(SP1, 0), slot(S, 1),
+                                     slot(SP1, 1), slot(S, 2), slot(SP1, 2), slot(SM1, 3),
+                                     slot(S, 3), slot(SP1, 3), p.o, cq2, cq1, cq3);
+            const PairSums qs = pair_sums(nb);
+            if (kin) {
+                ru = face_x<AP, BORDER>(nb, qs, p.g, a.use_div);
+                rv = face_y<AP, BORDER>(nb, qs, p.g, d, a.Vadv, p.j, k, a.pass, a.use_div);
+            }
+            rw = face_z<AP, BORDER>(nb, qs, p.g, k == 0, k == ns - 2, a.use_div);
+            c2 = nb.c_2;
+            cU = nb.cU;
+        }
+        const float2 dx = make_float2(flux(ru.x, cq2.x, cq2.y), flux(ru.y, cq2.y, c2));
+        const float2 dy = flux2(rv, cq2, cU);
+        const float2 dz = flux2(rw, cq2, cq3);  // face k+1/2
+        st2(sDX + p.w, dx);
+        st2(sDY + p.w, dy);
+        __syncthreads();
+        if (k >= z0 && k < z1) {
+            const long long q = p.col + (long long)k * pp;
+            if (p.ownA || p.ownB) {
+                const float2 netx = make_float2(dx.x - sDX[p.w - 1], dx.y - dx.x);
+                const float2 nety = dy - ld2(sDY + p.w - WX);
+                store_pair(a.c_out + q, cq2 - ((netx + nety) + (dz - dz_prev)), p.ownA, p.ownB);
+            }
+            if (a.write_faces) {
+                if (p.wxA) a.Un[q] = ru.x;
+                if (p.wxB) a.Un[q + 1] = ru.y;
+                if (p.wyA) a.Vn[q] = rv.x;
+                if (p.wyB) a.Vn[q + 1] = rv.y;
+                store_pair(a.Wn + q, rw, p.ownA, p.ownB);
+            }
+        } else if (k == 0 && z0 == 1 && a.write_faces) {  // face-plane 0 (below plane 1)
+            store_pair(a.Wn + p.col, rw, p.ownA, p.ownB);
+        }
+        dz_prev = dz;
+        cq1 = cq2;
+        cq2 = cq3;
+    };
+    for (int kb = kstart & ~(NSTAGE - 1); kb <= last; kb += NSTAGE) {
+        if (kb >= kstart) plane(IC<0>{}, kb);
+        if (kb + 1 >= kstart && kb + 1 <= last) plane(IC<1>{}, kb + 1);
+        if (kb + 2 >= kstart && kb + 2 <= last) plane(IC<2>{}, kb + 2);
+        if (kb + 3 >= kstart && kb + 3 <= last) plane(IC<3>{}, kb + 3);
+    }
+
+    if (!ok && a.err) atomicOr(a.err, 1);
+    if (tid == 0) {  // never leave with a copy in flight
+        for (int pl = confirmed; pl <= issue_max; pl++)
+            if (!tma::mbar_wait(&bars[pl & (NSTAGE - 1)], ((pl - kstart) / NSTAGE) & 1)) break;
+    }
+}
+
+// ---- with the limiter ----
+// Iteration k: [limited faces of plane k-1 and z face k-3/2, donor fluxes,
+// update of plane k-2; raw faces of plane k and z face k+1/2 with their
+// limiter fluxes and the bound extrema of plane k] -> sync -> [ratios of
+// plane k] -> sync.  Ratios and donor fluxes live in two-slot rings (plane
+// parity), so two barriers per plane suffice.
+template <bool AP, bool BORDER>
+__device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<float>& a,
+                                               const CUtensorMap* map_c, const CUtensorMap* map_cn,
+                                               const CUtensorMap* map_uo, const CUtensorMap* map_vo,
+                                               const CUtensorMap* map_wo, unsigned char* smem,
+                                               int i0, int j0)
+{
+    using namespace pair;
+    constexpr int NARR = n_arrays<true>();  // c, Uo, Vo, Wo, c^n
+    constexpr int SB = stage_bytes();
+    constexpr int Y = SBX;
+    float* work = reinterpret_cast<float*>(smem + (size_t)NSTAGE * NARR * SB);
+    float* sFX = work;           // limiter fluxes through the raw x faces of plane k (A|B, B|x+2)
+    float* sFY = sFX + WPL;      // through the raw y faces
+    float* sMX = sFY + WPL;      // bound extrema max / min(c, c^n) of plane k
+    float* sMN = sMX + WPL;
+    float* sBU = sMN + WPL;      // ratios (clamped to <= 1), two slots by plane parity
+    float* sBD = sBU + 2 * WPL;
+    float* sDX = sBD + 2 * WPL;  // donor fluxes through the limited faces, two slots
+    float* sDY = sDX + 2 * WPL;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sDY + 2 * WPL);
+    const PairSetup p = pair_setup<true, BORDER>(d, a, i0, j0);
+    const int ns = d.ns;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+    // The ring cells at x = 31 and y = CY-1 bound over a neighbour outside the
+    // CTA: the edge threads take its c and c^n from the staged planes.
+    const bool edge_x = tx == TX - 1, edge_y = ty == CY - 1;
+    const long long pp = d.pp;
+
+    if (tid == 0) {
+        for (int s = 0; s < NSTAGE; s++) tma::mbar_init(&bars[s], 1);
+        tma::fence_barrier_init();
+        tma::prefetch_map(map_c);
+        tma::prefetch_map(map_cn);
+        tma::prefetch_map(map_uo);
+        tma::prefetch_map(map_vo);
+        tma::prefetch_map(map_wo);
+    }
+    __syncthreads();
+    auto slot = [&](int s, int arr) -> const float* {
+        return reinterpret_cast<const float*>(smem + (size_t)(s * NARR + arr) * SB);
+    };
+    auto issue = [&](int pl) {
+        const int s = pl & (NSTAGE - 1);
+        uint64_t* bar = &bars[s];
+        tma::fence_proxy_async_shared();
+        tma::mbar_arrive_expect_tx(bar, (uint32_t)(NARR * SBX * SBY * sizeof(float)));
+        tma::load_3d(const_cast<float*>(slot(s, 0)), map_c, p.gx0, p.gy0, pl, bar);
+        tma::load_3d(const_cast<float*>(slot(s, 1)), map_uo, p.gx0, p.gy0, pl, bar);
+        tma::load_3d(const_cast<float*>(slot(s, 2)), map_vo, p.gx0, p.gy0, pl, bar);
+        tma::load_3d(const_cast<float*>(slot(s, 3)), map_wo, p.gx0, p.gy0, pl, bar);
+        tma::load_3d(const_cast<float*>(slot(s, 4)), map_cn, p.gx0, p.gy0, pl, bar);
+    };
+
+    // z chunk: the update of plane u comes two iterations after its raw faces
+    // (the limited z face above u needs the ratios of u+1).  Three warm-up
+    // planes: the z face below, then the ratios below, then their limited face.
+    const int depth = a.zdepth > 0 ? a.zdepth : ns - 2;
+    const int z0 = 1 + (int)blockIdx.z * depth;
+    const int z1 = min(ns - 1, z0 + depth);
+    const int kstart = max(0, z0 - 3);
+    const int last_a = z1;      // last plane whose raw faces and ratios are formed
+    const int last = z1 + 1;    // last iteration (update of plane z1 - 1)
+    const int issue_max = min(ns - 1, last_a + 1);
 
     bool ok = true;
     int confirmed = kstart;
@@ -413,77 +567,113 @@ __device__ __forceinline__ void pair_march(const Dims& d, const PassArgs<float>&
     if (tid == 0 && ok) confirmed = kstart + 1;
 
     // state carried between planes (pairs of the own cells)
-    float2 cq1 = bc(0.f), cq2 = ok ? ld2(slot(kstart & (NSTAGE - 1), 0) + o) : bc(0.f), cq3 = bc(0.f);
-    const long long kp0 = (long long)kstart * pp;
-    float2 cn_next = LIM ? ldcn(kstart + 1, kp0 + pp) : bc(0.f);  // c^n of plane k+1
-    float cnR_cur = LIM ? ldcnR(kstart, kp0) : 0.f;  // edge threads: c^n of plane k at x+2 / y+1
-    float2 cnU_cur = LIM ? ldcnU(kstart, kp0) : bc(0.f);
-    float2 mx_m = bc(0.f), mn_m = bc(0.f);               // own bounds of plane k-1
-    float2 mx_0 = bc(0.f), mn_0 = bc(0.f);               // own bounds of plane k
-    if (LIM) {
-        const float2 cn0 = ldcn(kstart, kp0);
-        mx_0 = max2(cq2, cn0);
-        mn_0 = min2(cq2, cn0);
-    }
-    float2 bu_prev = bc(1.f), bd_prev = bc(1.f);  // own ratios of plane k-1
-    float2 rw_prev = bc(0.f), fz_prev = bc(0.f);  // raw z face k-1/2 and its limiter flux
-    float2 dx_prev = bc(0.f), dy_prev = bc(0.f);  // own donor fluxes (x: A|B, B|x+2; y) of plane k-1
-    float2 dz_prev = bc(0.f);                     // donor flux of the z face below
+    float2 cq0 = bc(0.f), cq1 = bc(0.f);  // c of planes k-2, k-1
+    float2 cq2 = ok ? ld2(slot(kstart & (NSTAGE - 1), 0) + p.o) : bc(0.f), cq3 = bc(0.f);
+    float2 ru_prev = bc(0.f), rv_prev = bc(0.f);  // raw x / y faces of plane k-1
+    float2 rw_prev = bc(0.f), rw_pp = bc(0.f);    // raw z faces k-1/2 and k-3/2
+    float2 dz_prev = bc(0.f);                     // donor flux through the limited z face k-5/2
 
     auto plane = [&](auto Sc, const int k) {
         constexpr int S = decltype(Sc)::value;
         constexpr int SM1 = (S + NSTAGE - 1) % NSTAGE, SP1 = (S + 1) % NSTAGE;
-        __syncthreads();
-        if (tid == 0 && k + 2 <= min(ns - 1, last + 1)) issue(k + 2);
-        const long long kp = (long long)k * pp;  // element offset of plane k
-        float2 cn_next2 = bc(0.f), cnU_next = bc(0.f);
-        float cnR_next = 0.f;
-        if (LIM) {
-            cn_next2 = ldcn(k + 2, kp + 2 * pp);
-            cnR_next = ldcnR(k + 1, kp + pp);
-            cnU_next = ldcnU(k + 1, kp + pp);
-        }
-        if (k + 1 <= ns - 1) {
-            if (ok) ok = tma::mbar_wait(&bars[SP1], ((k + 1 - kstart) / NSTAGE) & 1);
-            if (tid == 0 && ok) confirmed = k + 2;
-            cq3 = ld2(slot(SP1, 0) + o);
-        }
-        const bool kin = k >= 1 && k <= ns - 2;
+        constexpr int PK = S & 1, PM = (S + 1) & 1;  // ring slots of planes k (and k-2) / k-1
+        // (the previous iteration ended with a barrier: the slot plane k+2 reuses is free)
+        if (tid == 0 && k + 2 <= issue_max) issue(k + 2);
 
-        // ---- raw faces of plane k (z: face-plane k) ----
-        float2 ru = bc(0.f), rv = bc(0.f), rw = bc(0.f);
-        float c2 = 0.f;      // c at x+2 (row y, plane k)
-        float2 cU = bc(0.f); // c at y+1
-        if (k <= ns - 2) {
-            const PairNb nb = gather(slot(SM1, 0), slot(S, 0), slot(SP1, 0), slot(S, 1),
-                                     slot(SP1, 1), slot(S, 2), slot(SP1, 2), slot(SM1, 3),
-                                     slot(S, 3), slot(SP1, 3), o, cq2, cq1, cq3);
-            const PairSums qs = pair_sums(nb);
-            if (kin) {
-                ru = face_x<AP, BORDER>(nb, qs, g, a.use_div);
-                rv = face_y<AP, BORDER>(nb, qs, g, d, a.Vadv, j, k, a.pass, a.use_div);
+        // ---- limited faces of plane k-1 and z face k-3/2; update of plane k-2 ----
+        {
+            const float* bu1 = sBU + PM * WPL;  // ratios of plane k-1
+            const float* bd1 = sBD + PM * WPL;
+            const float2 bu = ld2(bu1 + p.w), bd = ld2(bd1 + p.w);
+            const float2 bu2 = ld2(sBU + PK * WPL + p.w), bd2 = ld2(sBD + PK * WPL + p.w);
+            float2 lu = ru_prev, lv = rv_prev;
+            lu.x = limit(ru_prev.x, bu.x, bd.x, bu.y, bd.y);
+            if (!edge_x) lu.y = limit(ru_prev.y, bu.y, bd.y, bu1[p.w + 2], bd1[p.w + 2]);
+            if (!edge_y) {
+                const float2 buU = ld2(bu1 + p.w + WX), bdU = ld2(bd1 + p.w + WX);
+                lv = make_float2(limit(rv_prev.x, bu.x, bd.x, buU.x, bdU.x),
+                                 limit(rv_prev.y, bu.y, bd.y, buU.y, bdU.y));
             }
-            rw = face_z<AP, BORDER>(nb, qs, g, k == 0, k == ns - 2, a.use_div);
-            c2 = nb.c_2; cU = nb.cU;
+            const float2 lw = make_float2(limit(rw_pp.x, bu2.x, bd2.x, bu.x, bd.x),
+                                          limit(rw_pp.y, bu2.y, bd2.y, bu.y, bd.y));
+            const float* cm = slot(SM1, 0);  // staged c of plane k-1
+            const float c2m = cm[p.o + 2];
+            const float2 cUm = ld2(cm + p.o + Y);
+            const float2 dx = make_float2(flux(lu.x, cq1.x, cq1.y), flux(lu.y, cq1.y, c2m));
+            const float2 dy = flux2(lv, cq1, cUm);
+            const float2 dz = flux2(lw, cq0, cq1);  // face k-3/2
+            st2(sDX + PM * WPL + p.w, dx);
+            st2(sDY + PM * WPL + p.w, dy);
+            const long long q1 = p.col + (long long)(k - 1) * pp;  // plane k-1
+            if (a.write_faces) {
+                if (k - 1 >= z0 && k - 1 < z1) {
+                    if (p.wxA) a.Un[q1] = lu.x;
+                    if (p.wxB) a.Un[q1 + 1] = lu.y;
+                    if (p.wyA) a.Vn[q1] = lv.x;
+                    if (p.wyB) a.Vn[q1 + 1] = lv.y;
+                }
+                // face-plane k-2: the high face of plane k-2, and face-plane 0 in the first chunk
+                if (k >= 2 && k - 2 < z1 && (k - 2 >= z0 || k - 2 == 0))
+                    store_pair(a.Wn + (q1 - pp), lw, p.ownA, p.ownB);
+            }
+            const int u = k - 2;
+            if (u >= z0 && u < z1 && (p.ownA || p.ownB)) {
+                const float* dxp = sDX + PK * WPL;  // donor fluxes of plane k-2
+                const float* dyp = sDY + PK * WPL;
+                const float2 dxo = ld2(dxp + p.w);
+                const float2 netx = make_float2(dxo.x - dxp[p.w - 1], dxo.y - dxo.x);
+                const float2 nety = ld2(dyp + p.w) - ld2(dyp + p.w - WX);
+                store_pair(a.c_out + (q1 - pp), cq0 - ((netx + nety) + (dz - dz_prev)), p.ownA,
+                           p.ownB);
+            }
+            dz_prev = dz;
         }
 
-        if constexpr (LIM) {
-            // own bounds of plane k+1 (c^(o) and c^n)
-            const float2 mx_p = max2(cq3, cn_next), mn_p = min2(cq3, cn_next);
-            // limiter fluxes of the own high faces
-            const float fxI = flux(ru.x, cq2.x, cq2.y), fxH = flux(ru.y, cq2.y, c2);
-            const float2 fyH = flux2(rv, cq2, cU), fzH = flux2(rw, cq2, cq3);
-            st2(sFX + w, make_float2(fxI, fxH));
-            st2(sFY + w, fyH);
-            st2(sMX + w, mx_0);
-            st2(sMN + w, mn_0);
-            __syncthreads();
+        // ---- raw faces of plane k (z: face k+1/2), limiter fluxes, bound extrema ----
+        const bool kin = k >= 1 && k <= ns - 2;
+        float2 ru = bc(0.f), rv = bc(0.f), rw = bc(0.f), cU = bc(0.f);
+        float c2 = 0.f, fxI = 0.f, fxH = 0.f;
+        float2 fyH = bc(0.f), fzH = bc(0.f), mx0 = bc(0.f), mn0 = bc(0.f);
+        if (k <= last_a) {
+            if (k + 1 <= ns - 1) {
+                if (ok) ok = tma::mbar_wait(&bars[SP1], ((k + 1 - kstart) / NSTAGE) & 1);
+                if (tid == 0 && ok) confirmed = k + 2;
+                cq3 = ld2(slot(SP1, 0) + p.o);
+            }
+            if (k <= ns - 2) {
+                const PairNb nb = gather(slot(SM1, 0), slot(S, 0), slot(SP1, 0), slot(S, 1),
+                                         slot(SP1, 1), slot(S, 2), slot(SP1, 2), slot(SM1, 3),
+                                         slot(S, 3), slot(SP1, 3), p.o, cq2, cq1, cq3);
+                const PairSums qs = pair_sums(nb);
+                if (kin) {
+                    ru = face_x<AP, BORDER>(nb, qs, p.g, a.use_div);
+                    rv = face_y<AP, BORDER>(nb, qs, p.g, d, a.Vadv, p.j, k, a.pass, a.use_div);
+                }
+                rw = face_z<AP, BORDER>(nb, qs, p.g, k == 0, k == ns - 2, a.use_div);
+                c2 = nb.c_2;
+                cU = nb.cU;
+            }
+            fxI = flux(ru.x, cq2.x, cq2.y);
+            fxH = flux(ru.y, cq2.y, c2);
+            fyH = flux2(rv, cq2, cU);
+            fzH = flux2(rw, cq2, cq3);
+            const float2 cn0 = ld2(slot(S, 4) + p.o);
+            mx0 = max2(cq2, cn0);
+            mn0 = min2(cq2, cn0);
+            st2(sFX + p.w, make_float2(fxI, fxH));
+            st2(sFY + p.w, fyH);
+            st2(sMX + p.w, mx0);
+            st2(sMN + p.w, mn0);
+        }
+        __syncthreads();
 
-            // ---- ratios of plane k ----
+        // ---- ratios of plane k ----
+        if (k <= last_a) {
             float2 bu = bc(1.f), bd = bc(1.f);
             if (kin) {
-                const float fxL = sFX[w - 1];
-                const float2 fyL = ld2(sFY + w - WX);
+                const float fxL = sFX[p.w - 1];
+                const float2 fyL = ld2(sFY + p.w - WX);
+                const float2 fzL = flux2(rw_prev, cq1, cq2);  // raw z face k-1/2
                 // in: positive low-face and negative high-face fluxes; out: the rest
                 // (max(f,0) - f = max(-f,0)).  x lane-wise: A's faces are L|A and
                 // A|B, B's are A|B and B|x+2.
@@ -491,133 +681,59 @@ __device__ __forceinline__ void pair_march(const Dims& d, const PassArgs<float>&
                 const float2 finx = make_float2(pL + (pI - fxI), pI + (pH - fxH));
                 const float2 foutx = make_float2((pL - fxL) + pI, (pI - fxI) + pH);
                 const float2 z0v = bc(0.f);
-                const float2 py = max2(fyL, z0v), pz = max2(fz_prev, z0v);
+                const float2 py = max2(fyL, z0v), pz = max2(fzL, z0v);
                 const float2 hy = max2(fyH, z0v), hz = max2(fzH, z0v);
                 const float2 fin = finx + ((py + pz) + ((hy - fyH) + (hz - fzH)));
-                const float2 fout = foutx + (((py - fyL) + (pz - fz_prev)) + (hy + hz));
+                const float2 fout = foutx + (((py - fyL) + (pz - fzL)) + (hy + hz));
                 // bounds over the cell and its face neighbours (z only in 3D)
-                const float mAB = fmaxf(mx_0.x, mx_0.y), nAB = fminf(mn_0.x, mn_0.y);
-                const float2 mD = ld2(sMX + w - WX), nD = ld2(sMN + w - WX);
-                float2 mU, nU;
+                const float* cnS = slot(S, 4);
+                const float mAB = fmaxf(mx0.x, mx0.y), nAB = fminf(mn0.x, mn0.y);
                 float mR, nR;
-                if (edge_y) { mU = max2(cU, cnU_cur); nU = min2(cU, cnU_cur); }
-                else { mU = ld2(sMX + w + WX); nU = ld2(sMN + w + WX); }
-                if (edge_x) { mR = fmaxf(c2, cnR_cur); nR = fminf(c2, cnR_cur); }
-                else { mR = sMX[w + 2]; nR = sMN[w + 2]; }
-                float2 mx = make_float2(fmaxf(mAB, sMX[w - 1]), fmaxf(mAB, mR));
-                float2 mn = make_float2(fminf(nAB, sMN[w - 1]), fminf(nAB, nR));
-                mx = max2(mx, max2(mD, mU));
-                mn = min2(mn, min2(nD, nU));
+                if (edge_x) {
+                    const float cnR = cnS[p.o + 2];
+                    mR = fmaxf(c2, cnR);
+                    nR = fminf(c2, cnR);
+                } else {
+                    mR = sMX[p.w + 2];
+                    nR = sMN[p.w + 2];
+                }
+                float2 mU, nU;
+                if (edge_y) {
+                    const float2 cnU = ld2(cnS + p.o + Y);
+                    mU = max2(cU, cnU);
+                    nU = min2(cU, cnU);
+                } else {
+                    mU = ld2(sMX + p.w + WX);
+                    nU = ld2(sMN + p.w + WX);
+                }
+                float2 mx = make_float2(fmaxf(mAB, sMX[p.w - 1]), fmaxf(mAB, mR));
+                float2 mn = make_float2(fminf(nAB, sMN[p.w - 1]), fminf(nAB, nR));
+                mx = max2(mx, max2(ld2(sMX + p.w - WX), mU));
+                mn = min2(mn, min2(ld2(sMN + p.w - WX), nU));
                 if (ns > 3) {
-                    mx = max2(mx, max2(mx_m, mx_p));
-                    mn = min2(mn, min2(mn_m, mn_p));
+                    const float2 cnm = ld2(slot(SM1, 4) + p.o), cnp = ld2(slot(SP1, 4) + p.o);
+                    mx = max2(mx, max2(max2(cq1, cnm), max2(cq3, cnp)));
+                    mn = min2(mn, min2(min2(cq1, cnm), min2(cq3, cnp)));
                 }
                 const float2 eps = bc(FLT_MIN);
                 bu = min2(rat2<AP>(mx - cq2, fin + eps), bc(1.f));
                 bd = min2(rat2<AP>(cq2 - mn, fout + eps), bc(1.f));
                 if constexpr (BORDER) {
-                    bu = pick(g.cx, g.cy, bu, bc(1.f));
-                    bd = pick(g.cx, g.cy, bd, bc(1.f));
+                    bu = pick(p.g.cx, p.g.cy, bu, bc(1.f));
+                    bd = pick(p.g.cx, p.g.cy, bd, bc(1.f));
                 }
             }
-            st2(sBU + w, bu);
-            st2(sBD + w, bd);
-            __syncthreads();
-
-            // ---- limited faces: x, y of plane k; z of face-plane k-1 ----
-            float2 lu = ru, lv = rv;
-            lu.x = limit(ru.x, bu.x, bd.x, bu.y, bd.y);
-            if (tx < TX - 1) lu.y = limit(ru.y, bu.y, bd.y, sBU[w + 2], sBD[w + 2]);
-            if (ty < CY - 1) {
-                const float2 buU = ld2(sBU + w + WX), bdU = ld2(sBD + w + WX);
-                lv = make_float2(limit(rv.x, bu.x, bd.x, buU.x, bdU.x),
-                                 limit(rv.y, bu.y, bd.y, buU.y, bdU.y));
-            }
-            const float2 lw = make_float2(limit(rw_prev.x, bu_prev.x, bd_prev.x, bu.x, bd.x),
-                                          limit(rw_prev.y, bu_prev.y, bd_prev.y, bu.y, bd.y));
-            // donor fluxes of plane k (read by the neighbours' update one plane later)
-            const float2 dx_cur = make_float2(flux(lu.x, cq2.x, cq2.y), flux(lu.y, cq2.y, c2));
-            const float2 dy_cur = flux2(lv, cq2, cU);
-            const float2 dz = flux2(lw, cq1, cq2);  // face k-1/2
-            float* sDXk = sDX + (S & 1) * WPL;
-            float* sDYk = sDY + (S & 1) * WPL;
-            st2(sDXk + w, dx_cur);
-            st2(sDYk + w, dy_cur);
-            if (a.write_faces) {
-                const long long q = col + kp;
-                const bool mine_k = kin && k >= z0 && k < z1;
-                if (mine_k) {
-                    if (wxA) a.Un[q] = lu.x;
-                    if (wxB) a.Un[q + 1] = lu.y;
-                    if (wyA) a.Vn[q] = lv.x;
-                    if (wyB) a.Vn[q + 1] = lv.y;
-                }
-                if (k >= 1 && k - 1 < z1 && (k - 1 >= z0 || k - 1 == 0)) {
-                    if (ownA) a.Wn[q - pp] = lw.x;
-                    if (ownB) a.Wn[q - pp + 1] = lw.y;
-                }
-            }
-
-            // ---- donor update of plane k-1 ----
-            const int u = k - 1;
-            if (u >= z0 && u < z1 && (ownA || ownB)) {
-                const float* sDXp = sDX + (SM1 & 1) * WPL;
-                const float* sDYp = sDY + (SM1 & 1) * WPL;
-                const float2 netx = make_float2(dx_prev.x - sDXp[w - 1], dx_prev.y - dx_prev.x);
-                const float2 lowy = ld2(sDYp + w - WX);
-                const float2 cnew = cq1 - ((netx + (dy_prev - lowy)) + (dz - dz_prev));
-                float* out = a.c_out + (col + kp - pp);
-                if (ownA && ownB) st2(out, cnew);
-                else if (ownA) out[0] = cnew.x;
-                else out[1] = cnew.y;
-            }
-            mx_m = mx_0; mn_m = mn_0;
-            mx_0 = mx_p; mn_0 = mn_p;
-            bu_prev = bu; bd_prev = bd;
-            fz_prev = fzH;
-            dx_prev = dx_cur; dy_prev = dy_cur;
-            dz_prev = dz;
-        } else {
-            // donor fluxes of the raw faces of plane k
-            const float2 dx_cur = make_float2(flux(ru.x, cq2.x, cq2.y), flux(ru.y, cq2.y, c2));
-            const float2 dy_cur = flux2(rv, cq2, cU);
-            const float2 dz = flux2(rw, cq2, cq3);  // face k+1/2
-            st2(sDX + w, dx_cur);
-            st2(sDY + w, dy_cur);
-            __syncthreads();
-            if (k >= z0 && k < z1) {
-                const long long q = col + kp;
-                if (ownA || ownB) {
-                    const float2 netx = make_float2(dx_cur.x - sDX[w - 1], dx_cur.y - dx_cur.x);
-                    const float2 lowy = ld2(sDY + w - WX);
-                    const float2 cnew = cq2 - ((netx + (dy_cur - lowy)) + (dz - dz_prev));
-                    float* out = a.c_out + q;
-                    if (ownA && ownB) st2(out, cnew);
-                    else if (ownA) out[0] = cnew.x;
-                    else out[1] = cnew.y;
-                }
-                if (a.write_faces) {
-                    if (wxA) a.Un[q] = ru.x;
-                    if (wxB) a.Un[q + 1] = ru.y;
-                    if (wyA) a.Vn[q] = rv.x;
-                    if (wyB) a.Vn[q + 1] = rv.y;
-                    if (ownA) a.Wn[q] = rw.x;
-                    if (ownB) a.Wn[q + 1] = rw.y;
-                }
-            } else if (k == 0 && z0 == 1 && a.write_faces) {  // face-plane 0 (below plane 1)
-                if (ownA) a.Wn[col] = rw.x;
-                if (ownB) a.Wn[col + 1] = rw.y;
-            }
-            dz_prev = dz;
+            st2(sBU + PK * WPL + p.w, bu);
+            st2(sBD + PK * WPL + p.w, bd);
         }
-        rw_prev = rw;
+        __syncthreads();
+        cq0 = cq1;
         cq1 = cq2;
         cq2 = cq3;
-        if (LIM) {
-            cn_next = cn_next2;
-            cnR_cur = cnR_next;
-            cnU_cur = cnU_next;
-        }
+        ru_prev = ru;
+        rv_prev = rv;
+        rw_pp = rw_prev;
+        rw_prev = rw;
     };
     for (int kb = kstart & ~(NSTAGE - 1); kb <= last; kb += NSTAGE) {
         if (kb >= kstart) plane(IC<0>{}, kb);
@@ -628,17 +744,16 @@ __device__ __forceinline__ void pair_march(const Dims& d, const PassArgs<float>&
 
     if (!ok && a.err) atomicOr(a.err, 1);
     if (tid == 0) {  // never leave with a copy in flight
-        const int issued_last = min(ns - 1, last + 1);
-        for (int p = confirmed; p <= issued_last; p++)
-            if (!tma::mbar_wait(&bars[p & (NSTAGE - 1)], ((p - kstart) / NSTAGE) & 1)) break;
+        for (int pl = confirmed; pl <= issue_max; pl++)
+            if (!tma::mbar_wait(&bars[pl & (NSTAGE - 1)], ((pl - kstart) / NSTAGE) & 1)) break;
     }
 }
 
 template <bool LIM, bool AP>
 __global__ void __launch_bounds__(pair::NT, pair::NT >= 512 ? 1 : 2)
     k_pass_pair(Dims d, PassArgs<float> a, const __grid_constant__ CUtensorMap map_c,
-                const __grid_constant__ CUtensorMap map_uo, const __grid_constant__ CUtensorMap map_vo,
-                const __grid_constant__ CUtensorMap map_wo)
+                const __grid_constant__ CUtensorMap map_cn, const __grid_constant__ CUtensorMap map_uo,
+                const __grid_constant__ CUtensorMap map_vo, const __grid_constant__ CUtensorMap map_wo)
 {
     using namespace pair;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -647,10 +762,17 @@ __global__ void __launch_bounds__(pair::NT, pair::NT >= 512 ? 1 : 2)
     // CTAs whose every face is an interior face of the interior pattern take
     // the branch-free path (no boundary forms, no existence masks, no i = 1 column).
     const bool interior = i0 >= 2 && i0 + CX - 1 <= d.nx - 3 && j0 >= 1 && j0 + CY - 1 <= d.ny - 3;
-    if (interior)
-        pair_march<LIM, AP, false>(d, a, &map_c, &map_uo, &map_vo, &map_wo, smem, i0, j0);
-    else
-        pair_march<LIM, AP, true>(d, a, &map_c, &map_uo, &map_vo, &map_wo, smem, i0, j0);
+    if constexpr (LIM) {
+        if (interior)
+            pair_march_lim<AP, false>(d, a, &map_c, &map_cn, &map_uo, &map_vo, &map_wo, smem, i0, j0);
+        else
+            pair_march_lim<AP, true>(d, a, &map_c, &map_cn, &map_uo, &map_vo, &map_wo, smem, i0, j0);
+    } else {
+        if (interior)
+            pair_march_plain<AP, false>(d, a, &map_c, &map_uo, &map_vo, &map_wo, smem, i0, j0);
+        else
+            pair_march_plain<AP, true>(d, a, &map_c, &map_uo, &map_vo, &map_wo, smem, i0, j0);
+    }
 }
 
 template <bool LIM, bool AP>
@@ -667,12 +789,15 @@ int launch_pair_variant(const Dims& d, const PassArgs<float>& a, cudaStream_t s)
     dim3 g((d.nx - 2 + stride_x<LIM>() - 1) / stride_x<LIM>(),
            (d.ny - 2 + stride_y<LIM>() - 1) / stride_y<LIM>(), (d.ns - 2 + depth - 1) / depth);
     dim3 b(TX, CY);
-    k_pass_pair<LIM, AP><<<g, b, smem, s>>>(d, a, *a.maps2.c, *a.maps2.uo, *a.maps2.vo, *a.maps2.wo);
+    const CUtensorMap& cn = LIM ? *a.maps2.cn : *a.maps2.c;
+    k_pass_pair<LIM, AP><<<g, b, smem, s>>>(d, a, *a.maps2.c, cn, *a.maps2.uo, *a.maps2.vo,
+                                            *a.maps2.wo);
     return 1;
 }
 
 int launch_pass_pair(const Dims& d, const PassArgs<float>& a, cudaStream_t s)
 {
-    if (a.limiter) return a.approx ? launch_pair_variant<true, true>(d, a, s) : launch_pair_variant<true, false>(d, a, s);
+    if (a.limiter)
+        return a.approx ? launch_pair_variant<true, true>(d, a, s) : launch_pair_variant<true, false>(d, a, s);
     return a.approx ? launch_pair_variant<false, true>(d, a, s) : launch_pair_variant<false, false>(d, a, s);
 }

@@ -75,7 +75,7 @@ mpdata_options env_options()
     o.limiter = has("limiter");
     o.precision_form = has("precision_form");
     o.strict = has("strict");
-    o.kernel = has("unfused") ? 1 : (has("single") ? 2 : 0);
+    o.kernel = has("unfused") ? 1 : has("single") ? 2 : has("pair") ? 3 : 0;
     o.vv_fix = has("vv_fix");
     o.div_mode = has("div_off") ? MPDATA_DIV_OFF : MPDATA_DIV_REFERENCE;
     o.approx_div = has("approx_div");
@@ -333,7 +333,7 @@ int mpdata_set_default_options(const mpdata_options* opts)
         memset(&g_opts, 0, sizeof g_opts);
         return 0;
     }
-    if (opts->kernel < 0 || opts->kernel > 2 || opts->div_mode < 0 || opts->div_mode > 1)
+    if (opts->kernel < 0 || opts->kernel > 3 || opts->div_mode < 0 || opts->div_mode > 1)
         return mpd::fail(MPDATA_ERR_ARG, "bad option value");
     g_opts = *opts;
     return 0;

@@ -480,7 +480,9 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     if (opts) o = *opts;
     if (o.precision_form && dtype != MPDATA_F32)
         return fail(MPDATA_ERR_ARG, "precision_form applies to float storage only");
-    if (o.kernel < 0 || o.kernel > 2) return fail(MPDATA_ERR_ARG, "bad kernel option %d", o.kernel);
+    if (o.kernel < 0 || o.kernel > 3) return fail(MPDATA_ERR_ARG, "bad kernel option %d", o.kernel);
+    if (o.kernel == 3 && (dtype != MPDATA_F32 || o.strict || o.precision_form))
+        return fail(MPDATA_ERR_ARG, "the two-cell pass needs float storage without strict or precision_form");
     if (o.approx_div && (dtype != MPDATA_F32 || o.strict || o.kernel == 1))
         return fail(MPDATA_ERR_ARG, "approx_div needs float storage, fused kernels and no strict mode");
     std::unique_ptr<Solver> h(new Solver());
@@ -499,8 +501,8 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     // The two-cell pass: FP32, fast arithmetic, FP32 limiter ratios, fused kernels by
     // default.  With the limiter and IEEE division the one-cell pass is faster on B200
     // (the division slow paths spill the two-cell kernel's registers), so it keeps it.
-    h->pair = dtype == MPDATA_F32 && !o.strict && !o.precision_form && o.kernel == 0 &&
-              (o.approx_div || !o.limiter);
+    h->pair = o.kernel == 3 || (dtype == MPDATA_F32 && !o.strict && !o.precision_form &&
+                                o.kernel == 0 && (o.approx_div || !o.limiter));
     h->zdepth = default_zdepth(h.get());
     if (int rc = alloc_solver(h.get())) {
         free_solver(h.get());

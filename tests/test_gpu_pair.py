@@ -37,7 +37,7 @@ def _faces(case):
     return U.astype(np.float32), V.astype(np.float32), W.astype(np.float32)
 
 
-def _run(m, shape, order, opt, steps, approx=False, kernel=0, depth=None, seed=0):
+def _run(m, shape, order, opt, steps, approx=False, kernel=3, depth=None, seed=0):
     nx, ny, ns = shape
     case = workloads.random_case(nx, ny, ns, seed=seed)
     U, V, W = _faces(case)
@@ -70,7 +70,7 @@ def test_pair_pass_within_tolerance(m, approx, shape, order, opt):
 @pytest.mark.parametrize("shape", [(130, 100, 12), (67, 45, 9)], ids=lambda s: "x".join(map(str, s)))
 @pytest.mark.parametrize("opt", OPTS[:2], ids=lambda o: "-".join(o) or "plain")
 def test_pair_pass_agrees_with_one_cell_pass(m, shape, opt):
-    a, _ = _run(m, shape, 3, opt, 3, kernel=0, seed=5)
+    a, _ = _run(m, shape, 3, opt, 3, kernel=3, seed=5)
     b, _ = _run(m, shape, 3, opt, 3, kernel=2, seed=5)
     assert float(np.abs(a - b).max()) <= TOL
 
@@ -89,7 +89,7 @@ def test_pair_pass_limiter_positive_and_conservative(m):
     boundary CTAs): every cell stays >= 0, mass kept to 1e-6."""
     r = workloads.ring3d(n=96, ns=40, courant=0.4, wcourant=0.0, sigma=6.0, offset=20.0)
     U, V, W = (x.astype(np.float32) for x in workloads.faces_from_cells(r["u"], r["v"], r["w"]))
-    with m.Solver(96, 96, 40, order=3, limiter=True) as s:
+    with m.Solver(96, 96, 40, order=3, limiter=True, approx_div=True) as s:
         s.set_faces(U, V, W)
         s.set_field(r["c0"].astype(np.float32))
         m0 = s.mass()
@@ -111,7 +111,7 @@ def test_pair_pass_against_fp64_run(m, approx):
         s64.set_field(w["c0"])
         s64.step(10)
         ref = s64.get_field()
-    with m.Solver(160, 140, 24, order=3, limiter=True, approx_div=approx) as s32:
+    with m.Solver(160, 140, 24, order=3, limiter=True, approx_div=approx, kernel=3) as s32:
         s32.set_faces(*(w[k].astype(np.float32) for k in ("U", "V", "W")))
         s32.set_field(w["c0"].astype(np.float32))
         s32.step(10)
