@@ -57,6 +57,11 @@ struct mpdata_adjoint {
     std::vector<std::array<void*, 3>> lam_L;
     void* lam_R[3] = {nullptr, nullptr, nullptr};
     void* lam_B[2] = {nullptr, nullptr};
+    // The accumulators every adjoint step starts from zero (lam_lev[1..P-1],
+    // lam_L, then lam_R and lam_B) share one allocation, cleared by one memset
+    // per step; lam_R + lam_B are contiguous at its end.
+    void* zblock = nullptr;
+    size_t zblock_bytes = 0, zRB_bytes = 0;
     bool have_faces = false;
 };
 
@@ -141,9 +146,8 @@ int step_adj(mpdata_adjoint* h, mpdata_adjoint::Record& R, const T* lam_next, T*
     for (int o = 1; o < P; o++) L[o] = (T*)h->lam_lev[o];
     L[P] = (T*)lam_next;
     L[0] = lam_prev;
-    for (int o = 0; o < P; o++) CUDA_TRY(cudaMemsetAsync(L[o], 0, fb, h->stream));
-    for (int o = 1; o < P; o++)
-        for (int a = 0; a < 3; a++) CUDA_TRY(cudaMemsetAsync(h->lam_L[o][a], 0, fb, h->stream));
+    CUDA_TRY(cudaMemsetAsync(L[0], 0, fb, h->stream));
+    if (h->zblock) CUDA_TRY(cudaMemsetAsync(h->zblock, 0, h->zblock_bytes, h->stream));
     for (int o = P - 1; o >= 0; o--) {
         mpd::AdjPassArgs<T> a{};
         a.pass = o;
@@ -165,9 +169,8 @@ int step_adj(mpdata_adjoint* h, mpdata_adjoint::Record& R, const T* lam_next, T*
             a.RU = (const T*)R.R[o][0]; a.RV = (const T*)R.R[o][1]; a.RW = (const T*)R.R[o][2];
             a.bup = (const T*)R.B[o][0]; a.bdn = (const T*)R.B[o][1];
             if (h->opts.limiter) {
-                for (int k = 0; k < 3; k++) CUDA_TRY(cudaMemsetAsync(h->lam_R[k], 0, fb, h->stream));
-                CUDA_TRY(cudaMemsetAsync(h->lam_B[0], 0, fb, h->stream));
-                CUDA_TRY(cudaMemsetAsync(h->lam_B[1], 0, fb, h->stream));
+                // cleared with the block for the step's last pass; again for earlier passes
+                if (o != P - 1) CUDA_TRY(cudaMemsetAsync(h->lam_R[0], 0, h->zRB_bytes, h->stream));
                 a.lRU = (T*)h->lam_R[0]; a.lRV = (T*)h->lam_R[1]; a.lRW = (T*)h->lam_R[2];
                 a.lbup = (T*)h->lam_B[0]; a.lbdn = (T*)h->lam_B[1];
             }
@@ -302,15 +305,29 @@ int mpdata_adjoint_create(mpdata_adjoint_handle* out, int nx, int ny, int ns, in
         }
     }
     H->lam_lev.resize(order + 2);
-    for (auto& p : H->lam_lev)
-        if (!rc) rc = A(&p);
     H->lam_L.resize(order);
-    for (int o = 1; o < order && !rc; o++)
-        for (int a = 0; a < 3 && !rc; a++) rc = A(&H->lam_L[o][a]);
-    if (H->opts.limiter) {
-        for (int a = 0; a < 3 && !rc; a++) rc = A(&H->lam_R[a]);
-        for (int a = 0; a < 2 && !rc; a++) rc = A(&H->lam_B[a]);
+    const size_t fb = field_bytes(H);
+    const int nz = 4 * (order - 1) + (H->opts.limiter ? 5 : 0);
+    if (!rc && nz > 0) {
+        if (cudaMalloc(&H->zblock, nz * fb) != cudaSuccess) {
+            rc = mpd::fail(MPDATA_ERR_CUDA, "adjoint allocation failed");
+        } else {
+            H->blocks.push_back(H->zblock);
+            H->zblock_bytes = nz * fb;
+            char* z = (char*)H->zblock;
+            for (int o = 1; o < order; o++) { H->lam_lev[o] = z; z += fb; }
+            for (int o = 1; o < order; o++)
+                for (int a = 0; a < 3; a++) { H->lam_L[o][a] = z; z += fb; }
+            if (H->opts.limiter) {
+                H->zRB_bytes = 5 * fb;
+                for (int a = 0; a < 3; a++) { H->lam_R[a] = z; z += fb; }
+                for (int a = 0; a < 2; a++) { H->lam_B[a] = z; z += fb; }
+            }
+        }
     }
+    if (!rc) rc = A(&H->lam_lev[0]);
+    if (!rc) rc = A(&H->lam_lev[order]);
+    if (!rc) rc = A(&H->lam_lev[order + 1]);
     if (rc) {
         destroy(h.release());
         return rc == MPDATA_ERR_CUDA ? mpd::fail(MPDATA_ERR_NOMEM, "adjoint allocation failed") : rc;

@@ -20,16 +20,13 @@ void launch_pass_record(const Dims& d, const PassArgs<T>& a, T* RU, T* RV, T* RW
     dim3 g((d.nx + 31) / 32, (d.ny + 7) / 8, d.ns), b(32, 8);
     k_antidiff<T><<<g, b, 0, s>>>(d, a.c, a.Uo, a.Vo, a.Wo, a.Vadv, RU, RV, RW, a.pass, a.use_div,
                                   a.vv_fix);
-    const size_t fb = (size_t)d.pp * d.ns * sizeof(T);
     if (a.limiter) {
         if (a.wide)
             k_fct_beta<T, double><<<g, b, 0, s>>>(d, a.c, a.cn, RU, RV, RW, bup, bdn);
         else
             k_fct_beta<T, T><<<g, b, 0, s>>>(d, a.c, a.cn, RU, RV, RW, bup, bdn);
-        cudaMemcpyAsync(a.Un, RU, fb, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(a.Vn, RV, fb, cudaMemcpyDeviceToDevice, s);
-        cudaMemcpyAsync(a.Wn, RW, fb, cudaMemcpyDeviceToDevice, s);
-        k_fct_apply<T><<<g, b, 0, s>>>(d, bup, bdn, a.Un, a.Vn, a.Wn);
+        // raw faces stay in R, the limited ones go to Un/Vn/Wn (every used face is written)
+        k_fct_apply<T><<<g, b, 0, s>>>(d, bup, bdn, RU, RV, RW, a.Un, a.Vn, a.Wn);
         k_donor<T><<<g, b, 0, s>>>(d, a.c, a.Un, a.Vn, a.Wn, a.c_out, 1);
     } else {
         k_donor<T><<<g, b, 0, s>>>(d, a.c, RU, RV, RW, a.c_out, 1);
@@ -81,7 +78,7 @@ int launch_pass_unfused(const Dims& d, const PassArgs<T>& a, T* bup, T* bdn, cud
             k_fct_beta<T, double><<<g, b, 0, s>>>(d, a.c, a.cn, a.Un, a.Vn, a.Wn, bup, bdn);
         else
             k_fct_beta<T, T><<<g, b, 0, s>>>(d, a.c, a.cn, a.Un, a.Vn, a.Wn, bup, bdn);
-        k_fct_apply<T><<<g, b, 0, s>>>(d, bup, bdn, a.Un, a.Vn, a.Wn);
+        k_fct_apply<T><<<g, b, 0, s>>>(d, bup, bdn, a.Un, a.Vn, a.Wn, a.Un, a.Vn, a.Wn);
         n += 2;
     }
     k_donor<T><<<g, b, 0, s>>>(d, a.c, a.Un, a.Vn, a.Wn, a.c_out, 1);

@@ -199,10 +199,11 @@ __global__ void k_fct_beta(Dims d, const T* __restrict__ c, const T* __restrict_
     bdn[q] = T((A(psi) - A(mn)) / (fout + lim_tiny<A>()));
 }
 
-// Apply the limiter to every used face; shell cells count as beta = 1.
+// Apply the limiter to every used face (raw faces Ui/Vi/Wi -> limited
+// U/V/W; in place when they alias); shell cells count as beta = 1.
 template <typename T>
 __global__ void k_fct_apply(Dims d, const T* __restrict__ bup, const T* __restrict__ bdn,
-                            T* __restrict__ U, T* __restrict__ V, T* __restrict__ W)
+                            const T* Ui, const T* Vi, const T* Wi, T* U, T* V, T* W)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -219,15 +220,15 @@ __global__ void k_fct_apply(Dims d, const T* __restrict__ bup, const T* __restri
     const bool kin = k >= 1 && k <= ns - 2, jin = j >= 1 && j <= ny - 2, iin = i >= 1 && i <= nx - 2;
     if (kin && jin && i <= nx - 2) {
         bool lo = in(i, j, k), hi = in(i + 1, j, k);
-        U[q] = limit_face(U[q], up(q, lo), dn(q, lo), up(q + X, hi), dn(q + X, hi));
+        U[q] = limit_face(Ui[q], up(q, lo), dn(q, lo), up(q + X, hi), dn(q + X, hi));
     }
     if (kin && iin && j <= ny - 2) {
         bool lo = in(i, j, k), hi = in(i, j + 1, k);
-        V[q] = limit_face(V[q], up(q, lo), dn(q, lo), up(q + Y, hi), dn(q + Y, hi));
+        V[q] = limit_face(Vi[q], up(q, lo), dn(q, lo), up(q + Y, hi), dn(q + Y, hi));
     }
     if (jin && iin && k <= ns - 2) {
         bool lo = in(i, j, k), hi = in(i, j, k + 1);
-        W[q] = limit_face(W[q], up(q, lo), dn(q, lo), up(q + Z, hi), dn(q + Z, hi));
+        W[q] = limit_face(Wi[q], up(q, lo), dn(q, lo), up(q + Z, hi), dn(q + Z, hi));
     }
 }
 
