@@ -3,6 +3,8 @@
 #include "launch.h"
 #include "tma.cuh"
 
+#include <type_traits>
+
 namespace mpd {
 namespace fast {
 #include "kernels_pair.cuh"

@@ -572,13 +572,21 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
     float2 ru_prev = bc(0.f), rv_prev = bc(0.f);  // raw x / y faces of plane k-1
     float2 rw_prev = bc(0.f), rw_pp = bc(0.f);    // raw z faces k-1/2 and k-3/2
     float2 dz_prev = bc(0.f);                     // donor flux through the limited z face k-5/2
+    long long qk = p.col + (long long)kstart * pp;  // element offset of the pair in plane k
 
+    // One iteration.  The last one (k = last_a + 1) only limits the faces of
+    // plane k-1 and updates plane k-2, and needs no barrier.  It runs the
+    // same compiled copy as every plane with the same stage slot (a separate
+    // copy could contract multiply-adds differently, and a z chunk updates
+    // its first plane in the last iteration), so chunked marches stay
+    // bit-identical to unchunked ones.
     auto plane = [&](auto Sc, const int k) {
         constexpr int S = decltype(Sc)::value;
+        const bool HA = k <= last_a;  // uniform over the CTA
         constexpr int SM1 = (S + NSTAGE - 1) % NSTAGE, SP1 = (S + 1) % NSTAGE;
         constexpr int PK = S & 1, PM = (S + 1) & 1;  // ring slots of planes k (and k-2) / k-1
         // (the previous iteration ended with a barrier: the slot plane k+2 reuses is free)
-        if (tid == 0 && k + 2 <= issue_max) issue(k + 2);
+        if (HA && tid == 0 && k + 2 <= issue_max) issue(k + 2);
 
         // ---- limited faces of plane k-1 and z face k-3/2; update of plane k-2 ----
         {
@@ -604,7 +612,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
             const float2 dz = flux2(lw, cq0, cq1);  // face k-3/2
             st2(sDX + PM * WPL + p.w, dx);
             st2(sDY + PM * WPL + p.w, dy);
-            const long long q1 = p.col + (long long)(k - 1) * pp;  // plane k-1
+            const long long q1 = qk - pp;  // plane k-1
             if (a.write_faces) {
                 if (k - 1 >= z0 && k - 1 < z1) {
                     if (p.wxA) a.Un[q1] = lu.x;
@@ -629,12 +637,12 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
             dz_prev = dz;
         }
 
+        if (!HA) return;
         // ---- raw faces of plane k (z: face k+1/2), limiter fluxes, bound extrema ----
         const bool kin = k >= 1 && k <= ns - 2;
-        float2 ru = bc(0.f), rv = bc(0.f), rw = bc(0.f), cU = bc(0.f);
-        float c2 = 0.f, fxI = 0.f, fxH = 0.f;
-        float2 fyH = bc(0.f), fzH = bc(0.f), mx0 = bc(0.f), mn0 = bc(0.f);
-        if (k <= last_a) {
+        float2 ru, rv, rw, cU, fyH, fzH, mx0, mn0;
+        float c2, fxI, fxH;
+        {
             if (k + 1 <= ns - 1) {
                 if (ok) ok = tma::mbar_wait(&bars[SP1], ((k + 1 - kstart) / NSTAGE) & 1);
                 if (tid == 0 && ok) confirmed = k + 2;
@@ -648,10 +656,15 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 if (kin) {
                     ru = face_x<AP, BORDER>(nb, qs, p.g, a.use_div);
                     rv = face_y<AP, BORDER>(nb, qs, p.g, d, a.Vadv, p.j, k, a.pass, a.use_div);
+                } else {
+                    ru = rv = bc(0.f);
                 }
                 rw = face_z<AP, BORDER>(nb, qs, p.g, k == 0, k == ns - 2, a.use_div);
                 c2 = nb.c_2;
                 cU = nb.cU;
+            } else {  // the top shell plane: no faces
+                ru = rv = rw = cU = bc(0.f);
+                c2 = 0.f;
             }
             fxI = flux(ru.x, cq2.x, cq2.y);
             fxH = flux(ru.y, cq2.y, c2);
@@ -668,7 +681,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
         __syncthreads();
 
         // ---- ratios of plane k ----
-        if (k <= last_a) {
+        {
             float2 bu = bc(1.f), bd = bc(1.f);
             if (kin) {
                 const float fxL = sFX[p.w - 1];
@@ -734,6 +747,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
         rv_prev = rv;
         rw_pp = rw_prev;
         rw_prev = rw;
+        qk += pp;
     };
     for (int kb = kstart & ~(NSTAGE - 1); kb <= last; kb += NSTAGE) {
         if (kb >= kstart) plane(IC<0>{}, kb);
