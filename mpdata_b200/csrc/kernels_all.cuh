@@ -1,5 +1,7 @@
 // Kernel set of one arithmetic mode.  Included by kernels_fast.cu and
 // kernels_strict.cu with MPD_NS defined as the mode's namespace.
+#include <algorithm>
+
 #include "launch.h"
 #include "tma.cuh"
 
@@ -63,7 +65,19 @@ template <typename T>
 void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W, T* c1,
                   int copy_shell, cudaStream_t s)
 {
-    k_donor<T><<<full_grid(d), dim3(kBX, kBY), 0, s>>>(d, c0, U, V, W, c1, copy_shell);
+    if (copy_shell) {
+        k_donor<T><<<full_grid(d), dim3(kBX, kBY), 0, s>>>(d, c0, U, V, W, c1, copy_shell);
+        return;
+    }
+    // vector march: 32 x 8 threads of 16 bytes each; z chunks so that the grid
+    // holds about four waves of eight 256-thread CTAs on each of 148 SMs
+    constexpr int N = 16 / (int)sizeof(T);
+    const int gx = (int)((d.px / N + 31) / 32), gy = (d.ny - 2 + 7) / 8;
+    const long long cols = (long long)gx * gy;
+    const long long chunks = std::max(1LL, (4LL * 148 * 8 + cols - 1) / cols);
+    const int depth = std::max(4, (int)((d.ns - 2 + chunks - 1) / chunks));
+    dim3 g(gx, gy, (d.ns - 2 + depth - 1) / depth);
+    k_donor_v<T><<<g, dim3(32, 8), 0, s>>>(d, c0, U, V, W, c1, depth);
 }
 
 template <typename T>

@@ -252,3 +252,66 @@ __global__ void k_donor(Dims d, const T* __restrict__ c0, const T* __restrict__ 
         c1[q] = c0[q];
     }
 }
+
+// 16 bytes of consecutive elements (4 floats / 2 doubles), moved as one vector.
+template <typename T> struct Vec16 {
+    static constexpr int N = 16 / (int)sizeof(T);
+    T v[N];
+};
+template <typename T> __device__ __forceinline__ Vec16<T> ld16(const T* p)
+{
+    Vec16<T> r;
+    *reinterpret_cast<uint4*>(r.v) = __ldg(reinterpret_cast<const uint4*>(p));
+    return r;
+}
+template <typename T> __device__ __forceinline__ void st16(T* p, const Vec16<T>& r)
+{
+    *reinterpret_cast<uint4*>(p) = *reinterpret_cast<const uint4*>(r.v);
+}
+
+// The same donor-cell pass, z-marching: each thread owns 16 bytes of a row
+// (4 FP32 / 2 FP64 cells) and steps them through a chunk of `depth` planes,
+// keeping the own column's c and z faces of neighbouring planes in
+// registers; rows and faces move as 16-byte vectors (row pitch and pitch
+// offsets are multiples of 16 bytes).  Shell cells of a vector keep their c0
+// value (bndcpy's copy, smolar.c:5-31, is the same value in every level);
+// shell rows and planes are not touched.  Same donor_update expression as
+// k_donor, so both give the same bits.
+template <typename T>
+__global__ void __launch_bounds__(256) k_donor_v(Dims d, const T* __restrict__ c0,
+                                                 const T* __restrict__ U, const T* __restrict__ V,
+                                                 const T* __restrict__ W, T* __restrict__ c1,
+                                                 int depth)
+{
+    constexpr int N = Vec16<T>::N;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i0 >= d.px || j > d.ny - 2) return;
+    const int k0 = 1 + (int)blockIdx.z * depth, k1 = min(d.ns - 1, k0 + depth);
+    const long long Y = d.px, Z = d.pp;
+    long long q = cell(d, i0, j, k0);
+    Vec16<T> cm = ld16(c0 + q - Z), cc = ld16(c0 + q), wm = ld16(W + q - Z);
+    for (int k = k0; k < k1; k++, q += Z) {
+        const Vec16<T> cp = ld16(c0 + q + Z), cd = ld16(c0 + q - Y), cu = ld16(c0 + q + Y);
+        const Vec16<T> u = ld16(U + q), v = ld16(V + q), vd = ld16(V + q - Y), w = ld16(W + q);
+        // x neighbours across the vector's edges (the previous / next row element
+        // at the row ends: in bounds, only used by shell cells, whose result is dropped)
+        const T cl = __ldg(c0 + q - 1), cr = __ldg(c0 + q + N), ul = __ldg(U + q - 1);
+        Vec16<T> out;
+#pragma unroll
+        for (int e = 0; e < N; e++) {
+            const int i = i0 + e;
+            const T left = e == 0 ? cl : cc.v[e > 0 ? e - 1 : 0];
+            const T right = e == N - 1 ? cr : cc.v[e < N - 1 ? e + 1 : 0];
+            const T uleft = e == 0 ? ul : u.v[e > 0 ? e - 1 : 0];
+            out.v[e] = (i >= 1 && i <= d.nx - 2)
+                           ? donor_update(cc.v[e], left, right, cd.v[e], cu.v[e], cm.v[e], cp.v[e],
+                                          u.v[e], uleft, v.v[e], vd.v[e], w.v[e], wm.v[e])
+                           : cc.v[e];
+        }
+        st16(c1 + q, out);
+        cm = cc;
+        cc = cp;
+        wm = w;
+    }
+}
