@@ -175,6 +175,13 @@ int mpdata_get_field(mpdata_handle h, void* c, int where);
 /* The field before the last pass of the latest step (what smolar() leaves in *c0). */
 int mpdata_get_previous(mpdata_handle h, void* c, int where);
 
+/* z-planes [k0, k0+nk) of the newest field as dense nx*ny planes (halo
+ * exchange of z-slab decompositions).  get: host copies synchronise, device
+ * copies are queued on the handle's stream.  set: the planes are written into
+ * every field level (planes on the grid's own z boundary are shell). */
+int mpdata_get_planes(mpdata_handle h, int k0, int nk, void* dst, int where);
+int mpdata_set_planes(mpdata_handle h, int k0, int nk, const void* src, int where);
+
 /* Advance nsteps steps on the handle's stream (asynchronous). */
 int mpdata_step(mpdata_handle h, int nsteps);
 

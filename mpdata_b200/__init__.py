@@ -69,6 +69,8 @@ _lib.mpdata_set_field.argtypes = [_vp, _vp, C.c_int]
 _lib.mpdata_get_field.argtypes = [_vp, _vp, C.c_int]
 _lib.mpdata_get_previous.argtypes = [_vp, _vp, C.c_int]
 _lib.mpdata_step.argtypes = [_vp, C.c_int]
+_lib.mpdata_get_planes.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int]
+_lib.mpdata_set_planes.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int]
 _lib.mpdata_sync.argtypes = [_vp]
 _lib.mpdata_mass.argtypes = [_vp, C.POINTER(C.c_double)]
 _lib.mpdata_min.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
@@ -319,6 +321,20 @@ class Solver:
 
     def step(self, nsteps: int = 1):
         _check(_lib.mpdata_step(self._h, nsteps))
+
+    def get_planes(self, k0: int, nk: int, out=None):
+        """z-planes [k0, k0+nk) of the newest field (``mpdata_get_planes``);
+        ``out``: a host array or a CUDA tensor of shape (nk, ny, nx)."""
+        if out is None:
+            out = np.empty((nk,) + self.shape[1:], self.dtype)
+        p, where = _ptr(out, self.dtype)
+        _check(_lib.mpdata_get_planes(self._h, k0, nk, p, where))
+        return out
+
+    def set_planes(self, k0: int, planes):
+        """Overwrite z-planes [k0, k0+len) in every level (``mpdata_set_planes``)."""
+        p, where = _ptr(planes, self.dtype)
+        _check(_lib.mpdata_set_planes(self._h, k0, int(planes.shape[0]), p, where))
 
     def sync(self):
         _check(_lib.mpdata_sync(self._h))

@@ -722,6 +722,46 @@ int mpdata_step(mpdata_handle h, int nsteps)
     return mpd::step(reinterpret_cast<Solver*>(h), nsteps);
 }
 
+// z-planes [k0, k0 + nk) of the newest field, dense (nx x ny per plane).
+int mpdata_get_planes(mpdata_handle hh, int k0, int nk, void* dst, int where)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h || !dst || nk < 0 || k0 < 0 || k0 + nk > (h ? h->d.ns : 0))
+        return mpd::fail(MPDATA_ERR_ARG, "bad plane range");
+    if (!h->have_field) return mpd::fail(MPDATA_ERR_STATE, "no field set");
+    if (nk == 0) return 0;
+    if (int rc = ensure_device(h)) return rc;
+    const size_t w = (size_t)h->d.nx * h->esz;
+    const char* src = (const char*)h->c[h->cur] + (size_t)k0 * h->d.pp * h->esz;
+    CUDA_TRY(cudaMemcpy2DAsync(dst, w, src, (size_t)h->d.px * h->esz, w, (size_t)h->d.ny * nk,
+                               where == MPDATA_HOST ? cudaMemcpyDeviceToHost
+                                                    : cudaMemcpyDeviceToDevice,
+                               h->stream));
+    return where == MPDATA_HOST ? mpdata_sync(hh) : 0;
+}
+
+// Overwrite z-planes [k0, k0 + nk) in every field level (a plane on the
+// solver's own z boundary is shell, which every level carries; interior
+// planes of the other levels are rewritten by the passes before they are read).
+int mpdata_set_planes(mpdata_handle hh, int k0, int nk, const void* src, int where)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h || !src || nk < 0 || k0 < 0 || k0 + nk > (h ? h->d.ns : 0))
+        return mpd::fail(MPDATA_ERR_ARG, "bad plane range");
+    if (!h->have_field) return mpd::fail(MPDATA_ERR_STATE, "no field set");
+    if (nk == 0) return 0;
+    if (int rc = ensure_device(h)) return rc;
+    const size_t w = (size_t)h->d.nx * h->esz;
+    for (int b = 0; b < 3; b++) {
+        char* dst = (char*)h->c[b] + (size_t)k0 * h->d.pp * h->esz;
+        CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)h->d.px * h->esz, src, w, w, (size_t)h->d.ny * nk,
+                                   where == MPDATA_HOST ? cudaMemcpyHostToDevice
+                                                        : cudaMemcpyDeviceToDevice,
+                                   h->stream));
+    }
+    return where == MPDATA_HOST ? mpdata_sync(hh) : 0;
+}
+
 int mpdata_sync(mpdata_handle hh)
 {
     Solver* h = reinterpret_cast<Solver*>(hh);
