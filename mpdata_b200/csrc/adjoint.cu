@@ -111,7 +111,7 @@ void step_fwd(mpdata_adjoint* h, const T* in, T* out, mpdata_adjoint::Record* r)
     for (int o = 0; o < P; o++) {
         T* dst = (o == P - 1) ? out : (r ? (T*)R.lev[o + 1] : (T*)h->work[o & 1]);
         if (o == 0) {
-            mpd::fast::launch_donor<T>(d, lev_prev, Fu, Fv, Fw, dst, 1, h->stream);
+            mpd::fast::launch_donor<T>(d, lev_prev, Fu, Fv, Fw, dst, 1, 0, 0, h->stream);
         } else {
             mpd::PassArgs<T> a{};
             a.c = lev_prev;

@@ -55,29 +55,35 @@ inline dim3 full_grid(const Dims& d) { return dim3((d.nx + kBX - 1) / kBX, (d.ny
 template <typename T>
 void launch_courant(const Dims& d, const T* dx, const T* dy, const T* ds, T dt, const T* u0,
                     const T* u1, const T* v0, const T* v1, const T* w0, const T* w1, T* U,
-                    T* V, T* W, cudaStream_t s)
+                    T* V, T* W, int k0, int nk, cudaStream_t s)
 {
-    k_courant<T><<<full_grid(d), dim3(kBX, kBY), 0, s>>>(d, dx, dy, ds, dt, u0, u1, v0, v1, w0,
-                                                         w1, U, V, W);
+    if (nk <= 0) return;
+    dim3 g = full_grid(d);
+    g.z = nk;
+    k_courant<T><<<g, dim3(kBX, kBY), 0, s>>>(d, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, U, V, W,
+                                              k0);
 }
 
 template <typename T>
 void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W, T* c1,
-                  int copy_shell, cudaStream_t s)
+                  int copy_shell, int zb, int ze, cudaStream_t s)
 {
     if (copy_shell) {
         k_donor<T><<<full_grid(d), dim3(kBX, kBY), 0, s>>>(d, c0, U, V, W, c1, copy_shell);
         return;
     }
+    if (zb <= 0) zb = 1;
+    if (ze <= 0) ze = d.ns - 1;
+    if (ze <= zb) return;
     // vector march: 32 x 8 threads of 16 bytes each; z chunks so that the grid
     // holds about four waves of eight 256-thread CTAs on each of 148 SMs
     constexpr int N = 16 / (int)sizeof(T);
     const int gx = (int)((d.px / N + 31) / 32), gy = (d.ny - 2 + 7) / 8;
     const long long cols = (long long)gx * gy;
     const long long chunks = std::max(1LL, (4LL * 148 * 8 + cols - 1) / cols);
-    const int depth = std::max(4, (int)((d.ns - 2 + chunks - 1) / chunks));
-    dim3 g(gx, gy, (d.ns - 2 + depth - 1) / depth);
-    k_donor_v<T><<<g, dim3(32, 8), 0, s>>>(d, c0, U, V, W, c1, depth);
+    const int depth = std::max(4, (int)((ze - zb + chunks - 1) / chunks));
+    dim3 g(gx, gy, (ze - zb + depth - 1) / depth);
+    k_donor_v<T><<<g, dim3(32, 8), 0, s>>>(d, c0, U, V, W, c1, depth, zb, ze);
 }
 
 template <typename T>
@@ -102,9 +108,9 @@ int launch_pass_unfused(const Dims& d, const PassArgs<T>& a, T* bup, T* bdn, cud
 #define MPD_INSTANTIATE(T)                                                                  \
     template void launch_courant<T>(const Dims&, const T*, const T*, const T*, T, const T*, \
                                     const T*, const T*, const T*, const T*, const T*, T*,   \
-                                    T*, T*, cudaStream_t);                                  \
+                                    T*, T*, int, int, cudaStream_t);                        \
     template void launch_donor<T>(const Dims&, const T*, const T*, const T*, const T*, T*,  \
-                                  int, cudaStream_t);                                       \
+                                  int, int, int, cudaStream_t);                             \
     template int launch_pass_unfused<T>(const Dims&, const PassArgs<T>&, T*, T*,            \
                                         cudaStream_t);                                      \
     template int launch_pass_fused<T>(const Dims&, const PassArgs<T>&, cudaStream_t);

@@ -297,9 +297,10 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
     // earlier so every value the first updated plane reads is formed exactly
     // as an unchunked march would form it (2 planes of warm-up without the
     // limiter, 3 with it: the z faces below, then the ratios below).
-    const int depth = a.zdepth > 0 ? a.zdepth : ns - 2;
-    const int z0 = 1 + (int)blockIdx.z * depth;
-    const int z1 = min(ns - 1, z0 + depth);
+    const int zb = a.zbase > 0 ? a.zbase : 1, ze = a.zend > 0 ? a.zend : ns - 1;
+    const int depth = a.zdepth > 0 ? a.zdepth : ze - zb;
+    const int z0 = zb + (int)blockIdx.z * depth;
+    const int z1 = min(ze, z0 + depth);
     const int kstart = max(0, z0 - (LIM ? 3 : 2));
     const int last = LIM ? z1 : z1 - 1;  // iteration of the last update
 
@@ -474,9 +475,11 @@ int launch_fused_variant(const Dims& d, const PassArgs<T>& a, cudaStream_t s)
         configured = true;
     }
     constexpr int OW = LIM ? 1 : 0;
-    const int depth = a.zdepth > 0 ? a.zdepth : d.ns - 2;
+    const int zb = a.zbase > 0 ? a.zbase : 1, ze = a.zend > 0 ? a.zend : d.ns - 1;
+    if (ze <= zb) return 0;
+    const int depth = a.zdepth > 0 ? a.zdepth : ze - zb;
     dim3 g((d.nx - 2 + BX - 2 * OW - 1) / (BX - 2 * OW), (d.ny - 2 + BY - 2 * OW - 1) / (BY - 2 * OW),
-           (d.ns - 2 + depth - 1) / depth);
+           (ze - zb + depth - 1) / depth);
     dim3 b(BX, BY);
     const CUtensorMap& cn = LIM ? *a.maps.cn : *a.maps.c;
     k_pass_tma<T, LIM, A, AP><<<g, b, smem, s>>>(d, a, *a.maps.c, cn, *a.maps.uo, *a.maps.vo,

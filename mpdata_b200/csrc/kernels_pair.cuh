@@ -401,9 +401,10 @@ __device__ __forceinline__ void pair_march_plain(const Dims& d, const PassArgs<f
     };
 
     // z chunk (see k_pass_tma): two warm-up planes, the first for the z face below
-    const int depth = a.zdepth > 0 ? a.zdepth : ns - 2;
-    const int z0 = 1 + (int)blockIdx.z * depth;
-    const int z1 = min(ns - 1, z0 + depth);
+    const int zb = a.zbase > 0 ? a.zbase : 1, ze = a.zend > 0 ? a.zend : ns - 1;
+    const int depth = a.zdepth > 0 ? a.zdepth : ze - zb;
+    const int z0 = zb + (int)blockIdx.z * depth;
+    const int z1 = min(ze, z0 + depth);
     const int kstart = max(0, z0 - 2);
     const int last = z1 - 1;
     const int issue_max = min(ns - 1, last + 1);
@@ -549,9 +550,10 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
     // z chunk: the update of plane u comes two iterations after its raw faces
     // (the limited z face above u needs the ratios of u+1).  Three warm-up
     // planes: the z face below, then the ratios below, then their limited face.
-    const int depth = a.zdepth > 0 ? a.zdepth : ns - 2;
-    const int z0 = 1 + (int)blockIdx.z * depth;
-    const int z1 = min(ns - 1, z0 + depth);
+    const int zb = a.zbase > 0 ? a.zbase : 1, ze = a.zend > 0 ? a.zend : ns - 1;
+    const int depth = a.zdepth > 0 ? a.zdepth : ze - zb;
+    const int z0 = zb + (int)blockIdx.z * depth;
+    const int z1 = min(ze, z0 + depth);
     const int kstart = max(0, z0 - 3);
     const int last_a = z1;      // last plane whose raw faces and ratios are formed
     const int last = z1 + 1;    // last iteration (update of plane z1 - 1)
@@ -799,9 +801,11 @@ int launch_pair_variant(const Dims& d, const PassArgs<float>& a, cudaStream_t s)
         cudaFuncSetAttribute(k_pass_pair<LIM, AP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         configured = true;
     }
-    const int depth = a.zdepth > 0 ? a.zdepth : d.ns - 2;
+    const int zb = a.zbase > 0 ? a.zbase : 1, ze = a.zend > 0 ? a.zend : d.ns - 1;
+    if (ze <= zb) return 0;
+    const int depth = a.zdepth > 0 ? a.zdepth : ze - zb;
     dim3 g((d.nx - 2 + stride_x<LIM>() - 1) / stride_x<LIM>(),
-           (d.ny - 2 + stride_y<LIM>() - 1) / stride_y<LIM>(), (d.ns - 2 + depth - 1) / depth);
+           (d.ny - 2 + stride_y<LIM>() - 1) / stride_y<LIM>(), (ze - zb + depth - 1) / depth);
     dim3 b(TX, CY);
     const CUtensorMap& cn = LIM ? *a.maps2.cn : *a.maps2.c;
     k_pass_pair<LIM, AP><<<g, b, smem, s>>>(d, a, *a.maps2.c, cn, *a.maps2.uo, *a.maps2.vo,

@@ -15,11 +15,11 @@ __global__ void k_courant(Dims d, const T* __restrict__ dx, const T* __restrict_
                           const T* __restrict__ u1, const T* __restrict__ v0,
                           const T* __restrict__ v1, const T* __restrict__ w0,
                           const T* __restrict__ w1, T* __restrict__ U, T* __restrict__ V,
-                          T* __restrict__ W)
+                          T* __restrict__ W, int k0)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y * blockDim.y + threadIdx.y;
-    int k = blockIdx.z;
+    int k = k0 + (int)blockIdx.z;
     if (i >= d.nx || j >= d.ny) return;
     long long q = cell(d, i, j, k);
     const T quarter_dt = T(0.25) * dt;
@@ -281,13 +281,13 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_donor_v(Dims d, const T* __restrict__ c0,
                                                  const T* __restrict__ U, const T* __restrict__ V,
                                                  const T* __restrict__ W, T* __restrict__ c1,
-                                                 int depth)
+                                                 int depth, int zb, int ze)
 {
     constexpr int N = Vec16<T>::N;
     const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     if (i0 >= d.px || j > d.ny - 2) return;
-    const int k0 = 1 + (int)blockIdx.z * depth, k1 = min(d.ns - 1, k0 + depth);
+    const int k0 = zb + (int)blockIdx.z * depth, k1 = min(ze, k0 + depth);
     const long long Y = d.px, Z = d.pp;
     long long q = cell(d, i0, j, k0);
     Vec16<T> cm = ld16(c0 + q - Z), cc = ld16(c0 + q), wm = ld16(W + q - Z);

@@ -58,7 +58,8 @@ template <typename T> struct PassArgs {
     int wide;          // FP64 limiter ratios (float storage only)
     int write_faces;   // the next pass reads Un/Vn/Wn
     int approx;        // fused FP32 path: hardware-reciprocal ratios (approx_div form)
-    int zdepth;        // fused path: planes per CTA z chunk (0 = the whole column)
+    int zdepth;        // fused path: planes per CTA z chunk (0 = the whole range)
+    int zbase, zend;   // fused path: update planes [zbase, zend) only (0, 0: all interior planes)
 };
 
 // Ensemble (batched 2D instances): per-instance descriptor with the element
@@ -113,13 +114,15 @@ template <typename T> struct AdjPassArgs {
     template <typename T>                                                                  \
     int launch_ens_donor(int tile, T* arena, const EnsInst* insts, const EnsItem* items,   \
                          int nitems, int grid, const EnsPass& p, cudaStream_t s);          \
+    /* Faces of planes [k0, k0 + nk). */                                                   \
     template <typename T>                                                                  \
     void launch_courant(const Dims& d, const T* dx, const T* dy, const T* ds, T dt,        \
                         const T* u0, const T* u1, const T* v0, const T* v1, const T* w0,   \
-                        const T* w1, T* U, T* V, T* W, cudaStream_t s);                    \
+                        const T* w1, T* U, T* V, T* W, int k0, int nk, cudaStream_t s);    \
+    /* Pass 0 over interior planes [zb, ze) (0, 0: all); copy_shell: every plane. */       \
     template <typename T>                                                                  \
     void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W,      \
-                      T* c1, int copy_shell, cudaStream_t s);                              \
+                      T* c1, int copy_shell, int zb, int ze, cudaStream_t s);              \
     /* Corrective pass, one kernel per reference routine; bup/bdn scratch (limiter). */    \
     template <typename T>                                                                  \
     int launch_pass_unfused(const Dims& d, const PassArgs<T>& a, T* bup, T* bdn,           \

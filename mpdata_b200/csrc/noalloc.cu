@@ -99,7 +99,7 @@ extern "C" int mpdata_step_noalloc(int nx, int ny, int ns, int order, int limite
 
     // Pass o writes c_out when it is the last pass, else the level buffers in turn.
     auto dst = [&](int o) { return o == order - 1 ? c_out : lvl[o & 1]; };
-    mpd::fast::launch_donor<float>(d, c_in, U, V, W, dst(0), 1, s);
+    mpd::fast::launch_donor<float>(d, c_in, U, V, W, dst(0), 1, 0, 0, s);
     const float* in = dst(0);
     for (int o = 1; o < order; o++) {
         mpd::PassArgs<float> a{};

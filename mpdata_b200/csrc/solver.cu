@@ -307,7 +307,7 @@ template <typename T> int step_impl(Solver* h, int nsteps)
         {
             PassTimer t(h, 0);
             op.donor(d, Cb<T>(h, b0), F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), Cb<T>(h, b1), 0,
-                     h->stream);
+                     0, 0, h->stream);
         }
         int in = b1, out = b2;
         for (int o = 1; o < P; o++) {
@@ -336,6 +336,7 @@ template <typename T> int step_impl(Solver* h, int nsteps)
             a.write_faces = o < P - 1;
             a.approx = h->opts.approx_div;
             a.zdepth = h->zdepth;
+            a.zbase = a.zend = 0;  // every interior plane
             {
                 PassTimer timer(h, a.write_faces ? 1 : 2);
                 bool done = false;
@@ -553,13 +554,15 @@ int mpd::set_velocity(Solver* h, const void* dx, const void* dy, const void* ds,
         ops<float>(h).courant(h->d, m, m + h->d.nx, m + h->d.nx + h->d.ny, (float)dt,
                               (const float*)dev[0], (const float*)dev[1], (const float*)dev[2],
                               (const float*)dev[3], (const float*)dev[4], (const float*)dev[5],
-                              F<float>(h, 0, 0), F<float>(h, 0, 1), F<float>(h, 0, 2), h->stream);
+                              F<float>(h, 0, 0), F<float>(h, 0, 1), F<float>(h, 0, 2), 0,
+                              h->d.ns, h->stream);
     } else {
         const double* m = (const double*)h->metric;
         ops<double>(h).courant(h->d, m, m + h->d.nx, m + h->d.nx + h->d.ny, dt,
                                (const double*)dev[0], (const double*)dev[1], (const double*)dev[2],
                                (const double*)dev[3], (const double*)dev[4], (const double*)dev[5],
-                               F<double>(h, 0, 0), F<double>(h, 0, 1), F<double>(h, 0, 2), h->stream);
+                               F<double>(h, 0, 0), F<double>(h, 0, 1), F<double>(h, 0, 2), 0,
+                               h->d.ns, h->stream);
     }
     CUDA_TRY(cudaGetLastError());
     h->have_faces = true;
