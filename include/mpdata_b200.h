@@ -110,6 +110,15 @@ struct mpdata_options;
  * counterpart: the reference has no run-time options. */
 int mpdata_set_default_options(const struct mpdata_options* opts);
 
+/* smolar() / smolar_f64() on the calling thread: z planes per chunk of the
+ * pipelined host step (0: automatic, the default; < 0: no pipelining).  The
+ * pipelined step overlaps the uploads of the velocities and the field, the
+ * kernels and the downloads of both outputs chunk by chunk (with pinned host
+ * memory all copies are asynchronous); its results are the same bits as the
+ * unpipelined step.  Not with kernel=1 or check_courant (those step whole).
+ * No reference counterpart. */
+int mpdata_set_pipeline(int chunk_planes);
+
 /* ---- 2. Device-resident handle API ---------------------------------------- */
 
 typedef struct mpdata_solver* mpdata_handle;

@@ -80,6 +80,7 @@ _lib.mpdata_host_alloc.argtypes = [C.c_size_t]
 _lib.mpdata_host_free.argtypes = [_vp]
 _lib.msmolar_free.argtypes = [C.POINTER(_vp)]
 _lib.mpdata_set_default_options.argtypes = [C.POINTER(Options)]
+_lib.mpdata_set_pipeline.argtypes = [C.c_int]
 _lib.mpdata_ensemble_create.argtypes = [C.POINTER(_vp), C.c_int, C.POINTER(C.c_int),
                                         C.POINTER(C.c_int), C.c_int, C.POINTER(Options)]
 _lib.mpdata_ensemble_destroy.argtypes = [_vp]
@@ -123,6 +124,12 @@ def set_default_options(options: "SolverOptions | None" = None) -> None:
     else:
         o = options.to_c()
         _check(_lib.mpdata_set_default_options(C.byref(o)))
+
+
+def set_pipeline(chunk_planes: int = 0) -> None:
+    """z planes per chunk of the pipelined :func:`smolar` host step on the
+    calling thread (``mpdata_set_pipeline``): 0 automatic, < 0 no pipelining."""
+    _check(_lib.mpdata_set_pipeline(int(chunk_planes)))
 
 
 def _dtype_code(dtype) -> int:

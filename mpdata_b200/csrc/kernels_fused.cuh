@@ -407,7 +407,10 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
                 if (kin && mine_k && u_ok && oy && (ox || i == 0)) a.Un[q] = lu;
                 if (kin && mine_k && v_ok && ox && (oy || j == 0)) a.Vn[q] = lv;
                 // face-plane k-1: the high face of plane k-1, and face-plane 0 in the first chunk
-                if (k >= 1 && owned && k - 1 < z1 && (k - 1 >= z0 || k - 1 == 0)) a.Wn[q - d.pp] = lw;
+                // (face-plane 0 only from the chunk that starts at plane 1: a later
+                // chunk's warm-up does not form it)
+                if (k >= 1 && owned && k - 1 < z1 && (k - 1 >= z0 || (k - 1 == 0 && z0 == 1)))
+                    a.Wn[q - d.pp] = lw;
             }
 
             // ---- donor update of plane k-1 ----

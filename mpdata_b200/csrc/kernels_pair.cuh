@@ -622,8 +622,9 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                     if (p.wyA) a.Vn[q1] = lv.x;
                     if (p.wyB) a.Vn[q1 + 1] = lv.y;
                 }
-                // face-plane k-2: the high face of plane k-2, and face-plane 0 in the first chunk
-                if (k >= 2 && k - 2 < z1 && (k - 2 >= z0 || k - 2 == 0))
+                // face-plane k-2: the high face of plane k-2, and face-plane 0 only in
+                // the chunk that starts at plane 1 (a later chunk's warm-up does not form it)
+                if (k >= 2 && k - 2 < z1 && (k - 2 >= z0 || (k - 2 == 0 && z0 == 1)))
                     store_pair(a.Wn + (q1 - pp), lw, p.ownA, p.ownB);
             }
             const int u = k - 2;

@@ -84,6 +84,8 @@ mpdata_options env_options()
 }
 
 thread_local mpdata_options g_opts = env_options();
+// smolar(): planes per chunk of the pipelined host step (0 automatic, < 0 off).
+thread_local int g_pipe_chunk = 0;
 
 bool same_options(const mpdata_options& a, const mpdata_options& b)
 {
@@ -113,6 +115,20 @@ template <typename T> int smolar_host(int nx, int ny, int ns, T* dx, T* dy, T* d
     }
     h->order = order;
     const void* vel[6] = {u0, u1, v0, v1, w0, w1};
+    // Pipelined over z chunks (the default): the input *c0 is also an output
+    // buffer, which is safe because a chunk's planes come back only after the
+    // same planes have been uploaded and consumed.
+    if (g_pipe_chunk >= 0 && h->opts.kernel != 1 && !h->opts.check_courant) {
+        // the last pass writes the caller's c1 buffer when order is odd, c0 otherwise
+        T* newest = (order & 1) ? *c1 : *c0;
+        T* other = (order & 1) ? *c0 : *c1;
+        if (int rc = mpd::host_step_pipelined(h, dx, dy, ds, (double)dt, vel, *c0, newest, other,
+                                              g_pipe_chunk))
+            return rc;
+        *c1 = newest;
+        *c0 = other;
+        return 0;
+    }
     if (int rc = mpd::set_velocity(h, dx, dy, ds, (double)dt, vel, MPDATA_HOST)) return rc;
     if (int rc = mpd::set_field(h, *c0, MPDATA_HOST)) return rc;
     if (int rc = mpd::step(h, 1)) return rc;
@@ -326,6 +342,12 @@ template <typename T> int msmolar_gather_host(void** desc, T** c0, T** c1)
 }  // namespace
 
 extern "C" {
+
+int mpdata_set_pipeline(int chunk_planes)
+{
+    g_pipe_chunk = chunk_planes;
+    return 0;
+}
 
 int mpdata_set_default_options(const mpdata_options* opts)
 {

@@ -295,12 +295,58 @@ struct PassTimer {
     }
 };
 
+// Arguments of corrective pass o: input level `in`, output level `out`, step
+// input level b0 (limiter bounds); every interior plane unless narrowed.
+template <typename T> mpd::PassArgs<T> pass_args(Solver* h, int o, int in, int out, int b0)
+{
+    const int P = h->order;
+    const int rs = (o == 1) ? 0 : 1 + ((o - 2) & 1);  // face set read
+    const int ws = 1 + ((o - 1) & 1);                  // face set written
+    mpd::PassArgs<T> a{};
+    a.maps = {&h->tm_c[in], &h->tm_c[b0], &h->tm_f[rs][0], &h->tm_f[rs][1], &h->tm_f[rs][2]};
+    a.maps2 = {&h->tm2_c[in], &h->tm2_c[b0], &h->tm2_f[rs][0], &h->tm2_f[rs][1], &h->tm2_f[rs][2]};
+    a.err = h->dev_err;
+    a.c = Cb<T>(h, in);
+    a.cn = Cb<T>(h, b0);
+    a.Uo = F<T>(h, rs, 0);
+    a.Vo = F<T>(h, rs, 1);
+    a.Wo = F<T>(h, rs, 2);
+    a.Vadv = F<T>(h, 0, 1);
+    a.Un = F<T>(h, ws, 0);
+    a.Vn = F<T>(h, ws, 1);
+    a.Wn = F<T>(h, ws, 2);
+    a.c_out = Cb<T>(h, out);
+    a.pass = o;
+    a.use_div = h->opts.div_mode != MPDATA_DIV_OFF;
+    a.vv_fix = h->opts.vv_fix;
+    a.limiter = h->opts.limiter;
+    a.wide = h->opts.precision_form;
+    a.write_faces = o < P - 1;
+    a.approx = h->opts.approx_div;
+    a.zdepth = h->zdepth;
+    a.zbase = a.zend = 0;  // every interior plane
+    return a;
+}
+
+// Launch one corrective pass with the solver's kernel choice.
+template <typename T> void launch_pass(Solver* h, const mpd::PassArgs<T>& a, cudaStream_t s)
+{
+    if constexpr (std::is_same<T, float>::value) {
+        if (h->pair) {
+            mpd::fast::launch_pass_pair(h->d, a, s);
+            return;
+        }
+    }
+    ModeOps<T> op = ops<T>(h);
+    if (h->opts.kernel != 1) op.pass_fused(h->d, a, s);
+    else op.pass_unfused(h->d, a, (T*)h->bup, (T*)h->bdn, s);
+}
+
 template <typename T> int step_impl(Solver* h, int nsteps)
 {
     ModeOps<T> op = ops<T>(h);
     const Dims& d = h->d;
     const int P = h->order;
-    const bool fused = h->opts.kernel != 1;
     for (int s = 0; s < nsteps; s++) {
         const int b0 = h->cur, b1 = (b0 + 1) % 3, b2 = (b0 + 2) % 3;
         // pass 0: donor cell with the advective faces
@@ -311,45 +357,10 @@ template <typename T> int step_impl(Solver* h, int nsteps)
         }
         int in = b1, out = b2;
         for (int o = 1; o < P; o++) {
-            const int rs = (o == 1) ? 0 : 1 + ((o - 2) & 1);
-            const int ws = 1 + ((o - 1) & 1);
-            mpd::PassArgs<T> a;
-            a.maps = {&h->tm_c[in], &h->tm_c[b0], &h->tm_f[rs][0], &h->tm_f[rs][1], &h->tm_f[rs][2]};
-            a.maps2 = {&h->tm2_c[in], &h->tm2_c[b0], &h->tm2_f[rs][0], &h->tm2_f[rs][1],
-                       &h->tm2_f[rs][2]};
-            a.err = h->dev_err;
-            a.c = Cb<T>(h, in);
-            a.cn = Cb<T>(h, b0);
-            a.Uo = F<T>(h, rs, 0);
-            a.Vo = F<T>(h, rs, 1);
-            a.Wo = F<T>(h, rs, 2);
-            a.Vadv = F<T>(h, 0, 1);
-            a.Un = F<T>(h, ws, 0);
-            a.Vn = F<T>(h, ws, 1);
-            a.Wn = F<T>(h, ws, 2);
-            a.c_out = Cb<T>(h, out);
-            a.pass = o;
-            a.use_div = h->opts.div_mode != MPDATA_DIV_OFF;
-            a.vv_fix = h->opts.vv_fix;
-            a.limiter = h->opts.limiter;
-            a.wide = h->opts.precision_form;
-            a.write_faces = o < P - 1;
-            a.approx = h->opts.approx_div;
-            a.zdepth = h->zdepth;
-            a.zbase = a.zend = 0;  // every interior plane
+            const mpd::PassArgs<T> a = pass_args<T>(h, o, in, out, b0);
             {
                 PassTimer timer(h, a.write_faces ? 1 : 2);
-                bool done = false;
-                if constexpr (std::is_same<T, float>::value) {
-                    if (h->pair) {
-                        mpd::fast::launch_pass_pair(d, a, h->stream);
-                        done = true;
-                    }
-                }
-                if (!done) {
-                    if (fused) op.pass_fused(d, a, h->stream);
-                    else op.pass_unfused(d, a, (T*)h->bup, (T*)h->bdn, h->stream);
-                }
+                launch_pass<T>(h, a, h->stream);
             }
             int t = in; in = out; out = t;
         }
@@ -358,6 +369,151 @@ template <typename T> int step_impl(Solver* h, int nsteps)
     }
     CUDA_TRY(cudaGetLastError());
     return 0;
+}
+
+// One step of the host-array entry point, pipelined over z chunks.
+//
+// smolar() is bound by PCIe, not by the GPU: every call uploads the velocity
+// arrays and the field and downloads two fields.  Here the interior planes
+// are cut into chunks of D planes and three streams overlap the work:
+// the upload stream copies chunk i (velocities, field) and records an event;
+// the compute stream, once chunk i+1 has arrived, forms the faces of chunk i,
+// copies its planes of the input level into the other two levels (their
+// shell), runs pass 0 on chunk i and pass o on chunk i-o (a wavefront: pass o
+// on chunk j reads pass o-1 up to chunk j+1, and a chunk of >= 4 planes holds
+// every halo plane a pass reads); when the last pass has finished a chunk
+// the download stream copies its planes of the newest and the previous level
+// to the host.  Downloads overlap the later uploads (PCIe is full duplex) and
+// the kernels overlap both.  The kernels and their plane order are those of
+// the unchunked step (z-chunked marches give the same bits), so the result
+// equals step() on the whole grid bit for bit.  Pinned host memory lets every
+// copy run asynchronously; pageable memory gives the same result with less
+// overlap.
+template <typename T>
+int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const void* ds,
+                             double dt, const void* const vel[6], const void* c_in, void* newest,
+                             void* prev, int chunk)
+{
+    ModeOps<T> op = ops<T>(h);
+    const Dims& d = h->d;
+    const int ns = d.ns, P = h->order;
+    const size_t esz = h->esz, fb = field_bytes(h);
+    const int interior = ns - 2;
+    int D = chunk > 0 ? chunk : std::max(16, (interior + 7) / 8);
+    D = std::max(4, std::min(D, interior));
+    const int NC = (interior + D - 1) / D;
+    auto cb = [&](int i) { return 1 + i * D; };
+    auto ce = [&](int i) { return std::min(ns - 1, 1 + (i + 1) * D); };
+    auto ul = [&](int i) { return i == 0 ? 0 : cb(i); };        // upload / download range
+    auto uh = [&](int i) { return i == NC - 1 ? ns : ce(i); };
+
+    if (!h->s_up) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_up, cudaStreamNonBlocking));
+    if (!h->s_down) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_down, cudaStreamNonBlocking));
+    while ((int)h->pipe_ev.size() < 2 * NC + 1) {
+        cudaEvent_t e;
+        CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        h->pipe_ev.push_back(e);
+    }
+    cudaEvent_t* ev_up = h->pipe_ev.data();
+    cudaEvent_t* ev_done = ev_up + NC;
+    cudaEvent_t ev_start = ev_up[2 * NC];
+
+    // distinct velocity arrays (drivers pass the same array twice)
+    int src_of[6];
+    for (int v = 0; v < 6; v++) {
+        src_of[v] = v;
+        for (int w = 0; w < v; w++)
+            if (vel[w] == vel[v]) { src_of[v] = src_of[w]; break; }
+        if (src_of[v] == v && !h->vel[v]) CUDA_TRY(cudaMalloc(&h->vel[v], fb));
+    }
+    const T* dev[6];
+    for (int v = 0; v < 6; v++) dev[v] = (const T*)h->vel[src_of[v]];
+
+    // the upload stream may overwrite buffers only after earlier work on them
+    CUDA_TRY(cudaEventRecord(ev_start, h->stream));
+    CUDA_TRY(cudaStreamWaitEvent(h->s_up, ev_start, 0));
+    CUDA_TRY(cudaStreamWaitEvent(h->s_down, ev_start, 0));
+    char* met = (char*)h->metric;
+    CUDA_TRY(cudaMemcpyAsync(met, dx, d.nx * esz, cudaMemcpyHostToDevice, h->s_up));
+    CUDA_TRY(cudaMemcpyAsync(met + d.nx * esz, dy, d.ny * esz, cudaMemcpyHostToDevice, h->s_up));
+    CUDA_TRY(cudaMemcpyAsync(met + (d.nx + d.ny) * esz, ds, d.ns * esz, cudaMemcpyHostToDevice,
+                             h->s_up));
+    const size_t w = (size_t)d.nx * esz, plane_host = (size_t)d.nx * d.ny * esz;
+    const size_t plane_dev = (size_t)d.pp * esz;
+    auto up = [&](void* dst, const void* src, int k0, int k1) -> int {
+        CUDA_TRY(cudaMemcpy2DAsync((char*)dst + k0 * plane_dev, (size_t)d.px * esz,
+                                   (const char*)src + k0 * plane_host, w, w,
+                                   (size_t)d.ny * (k1 - k0), cudaMemcpyHostToDevice, h->s_up));
+        return 0;
+    };
+    auto down = [&](void* dst, const void* src, int k0, int k1) -> int {
+        CUDA_TRY(cudaMemcpy2DAsync((char*)dst + k0 * plane_host, w,
+                                   (const char*)src + k0 * plane_dev, (size_t)d.px * esz, w,
+                                   (size_t)d.ny * (k1 - k0), cudaMemcpyDeviceToHost, h->s_down));
+        return 0;
+    };
+    auto upload = [&](int i) -> int {
+        for (int v = 0; v < 6; v++)
+            if (src_of[v] == v)
+                if (int rc = up(h->vel[v], vel[v], ul(i), uh(i))) return rc;
+        if (int rc = up(h->c[0], c_in, ul(i), uh(i))) return rc;
+        CUDA_TRY(cudaEventRecord(ev_up[i], h->s_up));
+        return 0;
+    };
+
+    // levels: input 0; pass 0 writes 1, then the corrective passes alternate
+    const int b0 = 0, b1 = 1;
+    std::vector<int> lin(P), lout(P);
+    lout[0] = b1;
+    for (int o = 1; o < P; o++) {
+        lin[o] = lout[o - 1];
+        lout[o] = (o == 1) ? 2 : lin[o - 1];
+    }
+    const int cur = lout[P - 1], prv = (P == 1) ? b0 : lin[P - 1];
+    const T* m = (const T*)h->metric;
+
+    if (int rc = upload(0)) return rc;
+    if (NC > 1)
+        if (int rc = upload(1)) return rc;
+    for (int i = 0; i < NC + P - 1; i++) {
+        if (i + 2 < NC)
+            if (int rc = upload(i + 2)) return rc;
+        if (i < NC) {
+            CUDA_TRY(cudaStreamWaitEvent(h->stream, ev_up[std::min(i + 1, NC - 1)], 0));
+            op.courant(d, m, m + d.nx, m + d.nx + d.ny, (T)dt, dev[0], dev[1], dev[2], dev[3],
+                       dev[4], dev[5], F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), ul(i),
+                       uh(i) - ul(i), h->stream);
+            const size_t off = (size_t)ul(i) * plane_dev, len = (size_t)(uh(i) - ul(i)) * plane_dev;
+            for (int b = 1; b < 3; b++)
+                CUDA_TRY(cudaMemcpyAsync((char*)h->c[b] + off, (const char*)h->c[0] + off, len,
+                                         cudaMemcpyDeviceToDevice, h->stream));
+            op.donor(d, Cb<T>(h, b0), F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), Cb<T>(h, b1), 0,
+                     cb(i), ce(i), h->stream);
+        }
+        for (int o = 1; o < P; o++) {
+            const int j = i - o;
+            if (j < 0 || j >= NC) continue;
+            mpd::PassArgs<T> a = pass_args<T>(h, o, lin[o], lout[o], b0);
+            a.zbase = cb(j);
+            a.zend = ce(j);
+            if (a.zdepth >= D) a.zdepth = 0;  // the chunk in one march per column
+            launch_pass<T>(h, a, h->stream);
+        }
+        const int j = i - (P - 1);  // chunk the last pass has finished
+        if (j >= 0 && j < NC) {
+            CUDA_TRY(cudaEventRecord(ev_done[j], h->stream));
+            CUDA_TRY(cudaStreamWaitEvent(h->s_down, ev_done[j], 0));
+            if (int rc = down(newest, h->c[cur], ul(j), uh(j))) return rc;
+            if (int rc = down(prev, h->c[prv], ul(j), uh(j))) return rc;
+        }
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->s_down));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->cur = cur;
+    h->prev = prv;
+    h->have_field = h->have_faces = true;
+    return mpd::check_device_error(h);
 }
 
 template <typename T> int launches_per_step(const Solver* h)
@@ -454,6 +610,9 @@ void free_solver(Solver* h)
             cudaEventDestroy(p.second);
         }
     for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->pipe_ev) cudaEventDestroy(e);
+    if (h->s_up) cudaStreamDestroy(h->s_up);
+    if (h->s_down) cudaStreamDestroy(h->s_down);
     for (int b = 0; b < 3; b++) cudaFree(h->c[b]);
     for (int s = 0; s < 3; s++)
         for (int a = 0; a < 3; a++) cudaFree(h->faces[s][a]);
@@ -605,6 +764,20 @@ int mpd::get_field(Solver* h, void* c, int where, bool previous)
     if (!h->have_field) return fail(MPDATA_ERR_STATE, "no field set");
     if (int rc = ensure_device(h)) return rc;
     return get_grid(h, c, h->c[previous ? h->prev : h->cur], where);
+}
+
+int mpd::host_step_pipelined(Solver* h, const void* dx, const void* dy, const void* ds, double dt,
+                             const void* const vel[6], const void* c_in, void* newest, void* prev,
+                             int chunk)
+{
+    if (!h || !dx || !dy || !ds || !c_in || !newest || !prev) return fail(MPDATA_ERR_ARG, "null argument");
+    for (int v = 0; v < 6; v++)
+        if (!vel[v]) return fail(MPDATA_ERR_ARG, "null velocity array");
+    if (h->opts.kernel == 1) return fail(MPDATA_ERR_ARG, "the pipelined step needs the fused kernels");
+    if (int rc = ensure_device(h)) return rc;
+    return h->dtype == MPDATA_F32
+               ? host_step_pipelined_impl<float>(h, dx, dy, ds, dt, vel, c_in, newest, prev, chunk)
+               : host_step_pipelined_impl<double>(h, dx, dy, ds, dt, vel, c_in, newest, prev, chunk);
 }
 
 int mpd::step(Solver* h, int nsteps)

@@ -42,6 +42,9 @@ struct Solver {
     CUtensorMap tm2_f[3][3];
     bool have_field = false, have_faces = false;
     int zdepth = 0;  // fused kernels: planes per z chunk (set by the default heuristic / autotuner)
+    // Pipelined host-array step: upload and download streams, chunk events.
+    cudaStream_t s_up = nullptr, s_down = nullptr;
+    std::vector<cudaEvent_t> pipe_ev;
     // Optional per-pass event timing: pending event pairs per pass class.
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[3];
@@ -61,6 +64,12 @@ int set_faces(Solver* h, const void* U, const void* V, const void* W, int where)
 int set_field(Solver* h, const void* c, int where);
 int get_field(Solver* h, void* c, int where, bool previous);
 int step(Solver* h, int nsteps);
+// One step from host arrays (velocities vel[6], field c_in) to host arrays
+// (newest, prev: the field before the last pass), pipelined over z chunks of
+// `chunk` planes (0: automatic).  Fused kernels only.
+int host_step_pipelined(Solver* h, const void* dx, const void* dy, const void* ds, double dt,
+                        const void* const vel[6], const void* c_in, void* newest, void* prev,
+                        int chunk);
 int stats(Solver* h, double out[3]);
 int check_device_error(Solver* h);  // synchronises; reports a kernel's recorded error
 int launches(const Solver* h);

@@ -1,0 +1,86 @@
+"""The pipelined host step of smolar() (mpdata_set_pipeline).
+
+smolar() uploads velocities and field and downloads two fields on every
+call; the pipelined form overlaps those copies and the kernels chunk by
+chunk of z planes.  It runs the same kernels on the same planes, so its
+outputs must be the same bits as the unpipelined step's, for every chunk
+size, order, precision and option, over several driver-style calls (the
+newest output becomes the next input), with pageable and pinned host
+buffers.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from mpdata_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+NX, NY, NS = 37, 21, 40
+
+
+@pytest.fixture(scope="module")
+def m():
+    import mpdata_b200
+    yield mpdata_b200
+    mpdata_b200.set_pipeline(0)
+    mpdata_b200.set_default_options(None)
+
+
+def _run(m, f, order, chunk, steps, dtype, buffers=None):
+    m.set_pipeline(chunk)
+    c0 = f["c0"].astype(dtype).copy() if buffers is None else buffers[0]
+    c1 = np.zeros_like(c0) if buffers is None else buffers[1]
+    if buffers is not None:
+        c0[...] = f["c0"]
+        c1[...] = 0
+    outs = []
+    for _ in range(steps):
+        a, b = m.smolar(NX, NY, NS, f["dx"], f["dy"], f["ds"], f["dt"], f["u0"], f["u1"],
+                        f["v0"], f["v1"], f["w0"], f["w1"], c0, c1, order=order, dtype=dtype)
+        outs.append((a.copy(), b.copy()))
+        c0, c1 = b, a  # driver exchange: the newest field is the next input
+    return outs
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+@pytest.mark.parametrize("order", [1, 2, 3, 4])
+@pytest.mark.parametrize("opt", [dict(), dict(limiter=True), dict(limiter=True, strict=True),
+                                 dict(limiter=True, approx_div=True)],
+                         ids=["plain", "limiter", "strict", "approx"])
+def test_pipelined_smolar_same_bits(m, dtype, order, opt):
+    if opt.get("approx_div") and dtype is np.float64:
+        pytest.skip("approx_div is an FP32 form")
+    g = workloads.random_case(NX, NY, NS, seed=order + 3)
+    f = {k: (v.astype(dtype) if isinstance(v, np.ndarray) else v) for k, v in g.items()}
+    m.set_default_options(m.SolverOptions(**opt))
+    try:
+        ref = _run(m, f, order, -1, 3, dtype)
+        for chunk in (4, 5, 7, 0):
+            got = _run(m, f, order, chunk, 3, dtype)
+            for (ga, gb), (ra, rb) in zip(got, ref):
+                assert np.array_equal(ga, ra) and np.array_equal(gb, rb), chunk
+    finally:
+        m.set_default_options(None)
+
+
+def test_pipelined_smolar_pinned_buffers(m):
+    """Pinned host buffers (every copy asynchronous) give the same bits."""
+    g = workloads.random_case(NX, NY, NS, seed=17)
+    f = {k: (v.astype(np.float32) if isinstance(v, np.ndarray) else v) for k, v in g.items()}
+    lib = m.library()
+    n = NX * NY * NS
+    ptrs = [lib.mpdata_host_alloc(4 * n) for _ in range(2)]
+    try:
+        bufs = [np.ctypeslib.as_array((C.c_float * n).from_address(p)).reshape(NS, NY, NX)
+                for p in ptrs]
+        m.set_default_options(m.SolverOptions(limiter=True, approx_div=True))
+        ref = _run(m, f, 3, -1, 3, np.float32)
+        got = _run(m, f, 3, 6, 3, np.float32, buffers=bufs)
+        for (ga, gb), (ra, rb) in zip(got, ref):
+            assert np.array_equal(ga, ra) and np.array_equal(gb, rb)
+    finally:
+        m.set_default_options(None)
+        for p in ptrs:
+            lib.mpdata_host_free(C.c_void_p(p))
