@@ -399,7 +399,8 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
     const int ns = d.ns, P = h->order;
     const size_t esz = h->esz, fb = field_bytes(h);
     const int interior = ns - 2;
-    int D = chunk > 0 ? chunk : std::max(16, (interior + 7) / 8);
+    // 16 planes: measured best on B200 for a 512 x 512 plane (8: -3 %, 32: -8 %)
+    int D = chunk > 0 ? chunk : 16;
     D = std::max(4, std::min(D, interior));
     const int NC = (interior + D - 1) / D;
     auto cb = [&](int i) { return 1 + i * D; };
