@@ -71,7 +71,11 @@ KERNEL_OF_FORM = {
     "precision_form": "k_pass_tma<float, limiter, double ratios> (fused, one cell per thread)",
     "approx_div": "k_pass_pair<limiter, approx> (fused corrective pass, two cells per thread)",
 }
-CONFIG_TEXT = "roofline: 512x512x256 FP32, IORD 3 + nonoscillatory limiter, streamfunction flow"
+
+
+def config_text():
+    return (f"roofline: {NX}x{NY}x{NS} FP32, IORD {ORDER} + nonoscillatory limiter, "
+            "streamfunction flow")
 
 
 def hbm_peak():
@@ -377,7 +381,7 @@ def run_gpu(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": CONFIG_TEXT, "nx": NX, "ny": NY, "ns": NS, "order": ORDER,
+        "config": {"workload": config_text(), "nx": NX, "ny": NY, "ns": NS, "order": ORDER,
                    "limiter": True, "interior_cells": CELLS,
                    "l2": "inputs larger than L2 (268 MB per field); no flush",
                    "parallelism": f"replicas x{world} (one grid per GPU)" if world > 1 else "single GPU"},
@@ -643,7 +647,7 @@ def run_reference(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": cb["seconds"] / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": CONFIG_TEXT, "nx": NX, "ny": NY, "ns": NS, "order": ORDER,
+            "config": {"workload": config_text(), "nx": NX, "ny": NY, "ns": NS, "order": ORDER,
                        "limiter": False, "note": "the reference has no limiter"},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
