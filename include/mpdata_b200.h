@@ -47,6 +47,7 @@ extern "C" {
 #define MPDATA_ERR_NOMEM (-3)    /* device or host allocation failed */
 #define MPDATA_ERR_COURANT (-4)  /* |face Courant number| > 1 (when checking is on) */
 #define MPDATA_ERR_STATE (-5)    /* call out of order (e.g. step before set_field) */
+#define MPDATA_ERR_INT_DIV0 (-6) /* integer mode: a division by zero (the reference traps) */
 
 /* ---- 1. Reference-compatible entry points --------------------------------
  *
@@ -69,6 +70,16 @@ int smolar_f64(int nx, int ny, int ns, double* dx, double* dy, double* ds,
                const double dt, double* u0, double* u1, double* v0, double* v1,
                double* w0, double* w1, double** c0, double** c1, int flow_type,
                int order);
+
+/* Integer twin: the reference's smolar() built with -DINTEGER (real = long,
+ * smolar.h:14-16; ONE 4, HALF 2, QUAT 1, MINVAL 1, smolar_int.h:27-31), an
+ * exact-arithmetic mode.  Results equal that build's bit for bit while no
+ * value overflows 64 bits.  Where the reference would divide by zero (and
+ * trap) the call returns MPDATA_ERR_INT_DIV0 and leaves *c0, *c1 untouched.
+ * No limiter, no options; calls from several threads take turns. */
+int smolar_i64(int nx, int ny, int ns, long* dx, long* dy, long* ds, const long dt,
+               long* u0, long* u1, long* v0, long* v1, long* w0, long* w1, long** c0,
+               long** c1, int flow_type, int order);
 
 /* Decomposed step over an sx*sy*ss block grid.  *desc is created on the
  * first call (pass a NULL-initialised void*), holds the per-block device

@@ -33,7 +33,7 @@ HOST, DEVICE = 0, 1
 DIV_REFERENCE, DIV_OFF = 0, 1
 
 ERRORS = {-1: "MPDATA_ERR_ARG", -2: "MPDATA_ERR_CUDA", -3: "MPDATA_ERR_NOMEM",
-          -4: "MPDATA_ERR_COURANT", -5: "MPDATA_ERR_STATE"}
+          -4: "MPDATA_ERR_COURANT", -5: "MPDATA_ERR_STATE", -6: "MPDATA_ERR_INT_DIV0"}
 
 
 class MpdataError(RuntimeError):
@@ -142,7 +142,10 @@ def _dtype_code(dtype) -> int:
 
 
 def _ctype(dtype):
-    return C.c_float if np.dtype(dtype) == np.float32 else C.c_double
+    dt = np.dtype(dtype)
+    if dt == np.int64:
+        return C.c_long  # the reference's INTEGER build: real = long
+    return C.c_float if dt == np.float32 else C.c_double
 
 
 def _host_ptr(a: np.ndarray, dtype) -> C.c_void_p:
@@ -172,14 +175,18 @@ def _ptr(a, dtype):
 def smolar(nx, ny, ns, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, c0, c1,
            flow_type=DIVERGENT, order=2, dtype=np.float32):
     """One MPDATA step through the reference-compatible ``smolar()``
-    (``smolar_f64()`` for float64).
+    (``smolar_f64()`` for float64, ``smolar_i64()`` -- the reference's
+    INTEGER build -- for int64, where ``dt`` is an integer too).
 
     ``c0`` is the input field and both ``c0`` and ``c1`` are written.  Returns
     ``(c0, c1)`` the way the reference leaves ``*c0``/``*c1``: ``c1`` is the
     newest field, ``c0`` the field before the last pass (the two arrays trade
     places iff ``order`` is even, core/src/smolar.c:58)."""
-    fn = _lib.smolar if np.dtype(dtype) == np.float32 else _lib.smolar_f64
+    fn = {np.dtype(np.float32): _lib.smolar, np.dtype(np.float64): _lib.smolar_f64,
+          np.dtype(np.int64): _lib.smolar_i64}[np.dtype(dtype)]
     T = _ctype(dtype)
+    if np.dtype(dtype) == np.int64:
+        dt = int(dt)
     P = C.POINTER(T)
     pc0 = C.cast(c0.ctypes.data, P)
     pc1 = C.cast(c1.ctypes.data, P)

@@ -4,7 +4,8 @@
 // read against the reference line by line, it runs every formula exactly as
 // the fused kernels do but through global memory, one routine at a time.
 // Included by kernels_fast.cu / kernels_strict.cu inside namespace
-// mpd::MPD_NS.
+// mpd::MPD_NS, and by smolar_i64.cu (the reference's INTEGER build: the
+// same kernels on long long, constants from RealConst, truncating division).
 
 // Advective face Courant numbers (uu.c:126-138, vv.c:137-149, ww.c:143-155):
 //   U(i+1/2) = ((dt/4)/dx[i]) (((u0_i + u0_{i+1}) + u1_i) + u1_{i+1})
@@ -22,15 +23,15 @@ __global__ void k_courant(Dims d, const T* __restrict__ dx, const T* __restrict_
     int k = k0 + (int)blockIdx.z;
     if (i >= d.nx || j >= d.ny) return;
     long long q = cell(d, i, j, k);
-    const T quarter_dt = T(0.25) * dt;
+    const T quarter_dt = RealConst<T>::quat * dt;
     bool kin = k >= 1 && k <= d.ns - 2, jin = j >= 1 && j <= d.ny - 2, iin = i >= 1 && i <= d.nx - 2;
     T uf = T(0), vf = T(0), wf = T(0);
     if (kin && jin && i <= d.nx - 2)
-        uf = (quarter_dt / dx[i]) * (((u0[q] + u0[q + 1]) + u1[q]) + u1[q + 1]);
+        uf = ratio<false>(quarter_dt, dx[i]) * (((u0[q] + u0[q + 1]) + u1[q]) + u1[q + 1]);
     if (kin && iin && j <= d.ny - 2)
-        vf = (quarter_dt / dy[j]) * (((v0[q] + v0[q + d.px]) + v1[q]) + v1[q + d.px]);
+        vf = ratio<false>(quarter_dt, dy[j]) * (((v0[q] + v0[q + d.px]) + v1[q]) + v1[q + d.px]);
     if (jin && iin && k <= d.ns - 2)
-        wf = (quarter_dt / ds[k]) * (((w0[q] + w0[q + d.pp]) + w1[q]) + w1[q + d.pp]);
+        wf = ratio<false>(quarter_dt, ds[k]) * (((w0[q] + w0[q + d.pp]) + w1[q]) + w1[q + d.pp]);
     U[q] = uf;
     V[q] = vf;
     W[q] = wf;
@@ -62,11 +63,11 @@ __global__ void k_antidiff(Dims d, const T* __restrict__ c, const T* __restrict_
         T vb, wb, neg_div = T(0);
         if (i == 0 || i == nx - 2) {
             long long a = (i == 0) ? q + X : q;  // adjacent interior cell
-            vb = T(0.5) * (Vo[a - Y] + Vo[a]);
-            wb = T(0.5) * (Wo[a - Z] + Wo[a]);
+            vb = RealConst<T>::half * (Vo[a - Y] + Vo[a]);
+            wb = RealConst<T>::half * (Wo[a - Z] + Wo[a]);
         } else {
-            vb = T(0.25) * (((Vo[q + X - Y] + Vo[q + X]) + Vo[q]) + Vo[q - Y]);
-            wb = T(0.25) * (((Wo[q + X - Z] + Wo[q + X]) + Wo[q]) + Wo[q - Z]);
+            vb = RealConst<T>::quat * (((Vo[q + X - Y] + Vo[q + X]) + Vo[q]) + Vo[q - Y]);
+            wb = RealConst<T>::quat * (((Wo[q + X - Z] + Wo[q + X]) + Wo[q]) + Wo[q - Z]);
             if (use_div) {
                 T s = Uo[q + X] - Uo[q - X];
                 s = s + Vo[q + X - Y];
@@ -77,7 +78,7 @@ __global__ void k_antidiff(Dims d, const T* __restrict__ c, const T* __restrict_
                 s = s - Wo[q + X];
                 s = s - Wo[q];
                 s = s + Wo[q - Z];
-                neg_div = -((T(0.25) * Uo[q]) * s);
+                neg_div = -((RealConst<T>::quat * Uo[q]) * s);
             } else {
                 neg_div = -T(0);
             }
@@ -94,14 +95,14 @@ __global__ void k_antidiff(Dims d, const T* __restrict__ c, const T* __restrict_
         bool done = false;
         if (j == 0 || j == ny - 2) {
             long long a = (j == 0) ? q + Y : q;
-            ub = T(0.5) * (Uo[a - X] + Uo[a]);
-            wb = T(0.5) * (Wo[a - Z] + Wo[a]);
+            ub = RealConst<T>::half * (Uo[a - X] + Uo[a]);
+            wb = RealConst<T>::half * (Wo[a - Z] + Wo[a]);
         } else if (i == 1 && !vv_fix) {
             Vn[q] = (pass & 1) ? T(0) : Vadv[q];
             done = true;
         } else {
-            ub = T(0.25) * (((Uo[q - X + Y] + Uo[q + Y]) + Uo[q]) + Uo[q - X]);
-            wb = T(0.25) * (((Wo[q + Y - Z] + Wo[q + Y]) + Wo[q]) + Wo[q - Z]);
+            ub = RealConst<T>::quat * (((Uo[q - X + Y] + Uo[q + Y]) + Uo[q]) + Uo[q - X]);
+            wb = RealConst<T>::quat * (((Wo[q + Y - Z] + Wo[q + Y]) + Wo[q]) + Wo[q - Z]);
             if (use_div) {
                 T ul2u = (i >= 2) ? Uo[q - 2 * X + Y] : T(0);
                 T ul2 = (i >= 2) ? Uo[q - 2 * X] : T(0);
@@ -114,7 +115,7 @@ __global__ void k_antidiff(Dims d, const T* __restrict__ c, const T* __restrict_
                 s = s - ul2u;
                 s = s - ul2;
                 s = s + Uo[q - X];
-                neg_div = -((T(0.25) * Vo[q]) * s);
+                neg_div = -((RealConst<T>::quat * Vo[q]) * s);
             } else {
                 neg_div = -T(0);
             }
@@ -132,11 +133,11 @@ __global__ void k_antidiff(Dims d, const T* __restrict__ c, const T* __restrict_
         T ub, vb, neg_div = T(0);
         if (k == 0 || k == ns - 2) {
             long long a = (k == 0) ? q + Z : q;
-            ub = T(0.5) * (Uo[a - X] + Uo[a]);
-            vb = T(0.5) * (Vo[a - Y] + Vo[a]);
+            ub = RealConst<T>::half * (Uo[a - X] + Uo[a]);
+            vb = RealConst<T>::half * (Vo[a - Y] + Vo[a]);
         } else {
-            ub = T(0.25) * (((Uo[q] + Uo[q + Z]) + Uo[q - X + Z]) + Uo[q - X]);
-            vb = T(0.25) * (((Vo[q - Y + Z] + Vo[q + Z]) + Vo[q]) + Vo[q - Y]);
+            ub = RealConst<T>::quat * (((Uo[q] + Uo[q + Z]) + Uo[q - X + Z]) + Uo[q - X]);
+            vb = RealConst<T>::quat * (((Vo[q - Y + Z] + Vo[q + Z]) + Vo[q]) + Vo[q - Y]);
             if (use_div) {
                 T s = Wo[q + Z] - Wo[q - Z];
                 s = s + Uo[q - X + Z];
@@ -147,7 +148,7 @@ __global__ void k_antidiff(Dims d, const T* __restrict__ c, const T* __restrict_
                 s = s - Vo[q + Z];
                 s = s - Vo[q];
                 s = s + Vo[q - Y];
-                neg_div = -((T(0.25) * Wo[q]) * s);
+                neg_div = -((RealConst<T>::quat * Wo[q]) * s);
             } else {
                 neg_div = -T(0);
             }
@@ -155,7 +156,8 @@ __global__ void k_antidiff(Dims d, const T* __restrict__ c, const T* __restrict_
         T n1, d1, n2, d2;
         grad_pair(c[q + X + Z], c[q + X], c[q - X], c[q - X + Z], n1, d1);
         grad_pair(c[q + Y + Z], c[q + Y], c[q - Y], c[q - Y + Z], n2, d2);
-        Wn[q] = face_pattern(neg_div, Wo[q], c[q], c[q + Z], ub, n1, d1, vb, n2, d2);
+        Wn[q] = face_pattern<T, false, true>(neg_div, Wo[q], c[q], c[q + Z], ub, n1, d1, vb, n2,
+                                             d2);
     }
 }
 

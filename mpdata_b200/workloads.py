@@ -146,6 +146,32 @@ def random_case(nx, ny, ns, seed=0, courant=0.3, positive=True):
     return dict(u0=u0, u1=u1, v0=v0, v1=v1, w0=w0, w1=w1, c0=c, dx=dx, dy=dy, ds=ds, dt=0.9)
 
 
+def integer_case(nx, ny, ns, seed=0, cmax=40, moving=0.15):
+    """Inputs for the reference's INTEGER build (real = long): int64 arrays.
+    Grid steps 1 or 2 and dt 1 or 2 (so some faces truncate to 0: QUAT dt /
+    dx is an integer division), sparse cell velocities in {-1, 0, 1} (a
+    fraction `moving` of the cells, two time levels), a field of small
+    non-negative integers.  Values stay small over a few steps, but the
+    integer scheme is not positivity-preserving: a later step may divide by
+    zero (c_hi + c_lo + MINVAL = 0), which callers detect."""
+    rng = np.random.default_rng(seed)
+    sh = (ns, ny, nx)
+
+    def vel():
+        return np.where(rng.random(sh) < moving, rng.integers(-1, 2, sh), 0).astype(np.int64)
+
+    u0, v0, w0 = vel(), vel(), vel()
+    u1 = np.where(rng.random(sh) < 0.5, u0, vel()).astype(np.int64)
+    v1 = np.where(rng.random(sh) < 0.5, v0, vel()).astype(np.int64)
+    w1 = np.where(rng.random(sh) < 0.5, w0, vel()).astype(np.int64)
+    c = rng.integers(0, cmax + 1, sh).astype(np.int64)
+    dx = rng.integers(1, 3, nx).astype(np.int64)
+    dy = rng.integers(1, 3, ny).astype(np.int64)
+    ds = rng.integers(1, 3, ns).astype(np.int64)
+    return dict(u0=u0, u1=u1, v0=v0, v1=v1, w0=w0, w1=w1, c0=c, dx=dx, dy=dy, ds=ds,
+                dt=int(rng.integers(1, 3)))
+
+
 def ensemble(n: int = 256, lo: int = 64, hi: int = 512, seed: int = SEED + 4):
     """Batched-ensemble configuration: n independent 2D instances, NX, NY
     uniform in [lo, hi], solid-body rotation with max Courant uniform in

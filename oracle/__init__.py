@@ -75,7 +75,11 @@ def ref_lib(variant: str = "f32") -> C.CDLL:
 
 
 def _ct(dtype):
-    return C.c_float if np.dtype(dtype) == np.float32 else C.c_double
+    """C type of `real`: float, double, or long (the INTEGER build)."""
+    dt = np.dtype(dtype)
+    if dt == np.int64:
+        return C.c_long
+    return C.c_float if dt == np.float32 else C.c_double
 
 
 def _p(a: np.ndarray, dtype):
@@ -84,7 +88,10 @@ def _p(a: np.ndarray, dtype):
 
 
 def _sfx(dtype) -> str:
-    return "f32" if np.dtype(dtype) == np.float32 else "f64"
+    dt = np.dtype(dtype)
+    if dt == np.int64:
+        return "i64"
+    return "f32" if dt == np.float32 else "f64"
 
 
 def opts(limiter=0, vv_fix=0, div_mode=0, wide_beta=0) -> OracleOpts:
@@ -99,6 +106,7 @@ def _smolar_call(fn, dtype, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, c0, c1, orde
     T = _ct(dtype)
     pc0 = C.cast(c0.ctypes.data, C.POINTER(T))
     pc1 = C.cast(c1.ctypes.data, C.POINTER(T))
+    dt = int(dt) if np.dtype(dtype).kind == "i" else dt
     rc = fn(nx, ny, ns, _p(dx, dtype), _p(dy, dtype), _p(ds, dtype), T(dt),
             _p(u0, dtype), _p(u1, dtype), _p(v0, dtype), _p(v1, dtype), _p(w0, dtype),
             _p(w1, dtype), C.byref(pc0), C.byref(pc1), 1, order, *extra)
@@ -120,9 +128,10 @@ def smolar(dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, c0, c1, order, dtype=np.float
 
 
 def ref_smolar(dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, c0, c1, order, variant="f32"):
-    """The reference's own smolar() (compiled from its sources)."""
+    """The reference's own smolar() (compiled from its sources; variant 'i64'
+    is its INTEGER build)."""
     lib = ref_lib(variant)
-    dtype = np.float64 if variant == "f64" else np.float32
+    dtype = {"f64": np.float64, "i64": np.int64}.get(variant, np.float32)
     return _smolar_call(lib.smolar, dtype, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, c0, c1,
                         order)
 

@@ -85,6 +85,28 @@ void oracle_donor_f64(int nx, int ny, int ns, const double* c0, const double* U,
 double oracle_mass_f32(int nx, int ny, int ns, const float* c);
 double oracle_mass_f64(int nx, int ny, int ns, const double* c);
 
+/* The reference's INTEGER build (smolar.h:14-16: real = long; ONE 4, HALF 2,
+ * QUAT 1, MINVAL 1, core/include/smolar_int.h:27-31).  Same functions, C's
+ * truncating division; oracle_smolar_i64 returns -2 where the reference would
+ * divide by zero (and trap), -1 for the limiter (the mode has none). */
+void oracle_courant_i64(int nx, int ny, int ns, const long* dx, const long* dy,
+                        const long* ds, long dt, const long* u0, const long* u1,
+                        const long* v0, const long* v1, const long* w0, const long* w1,
+                        long* U, long* V, long* W);
+int oracle_step_faces_i64(int nx, int ny, int ns, const long* U, const long* V,
+                          const long* W, const long* c0, long* c1, long* inter, int order,
+                          const oracle_opts* opts);
+int oracle_smolar_i64(int nx, int ny, int ns, long* dx, long* dy, long* ds, const long dt,
+                      long* u0, long* u1, long* v0, long* v1, long* w0, long* w1,
+                      long** c0, long** c1, int flow_type, int order,
+                      const oracle_opts* opts);
+void oracle_antidiff_i64(int nx, int ny, int ns, const long* c, const long* Uo,
+                         const long* Vo, const long* Wo, const long* Vadv, int pass,
+                         long* Un, long* Vn, long* Wn, const oracle_opts* opts);
+void oracle_donor_i64(int nx, int ny, int ns, const long* c0, const long* U, const long* V,
+                      const long* W, long* c1);
+double oracle_mass_i64(int nx, int ny, int ns, const long* c);
+
 #ifdef __cplusplus
 }
 #endif

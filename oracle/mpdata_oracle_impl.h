@@ -1,7 +1,8 @@
 /* Precision-generic body of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
- * Included twice by mpdata_oracle.c with R = float / double, SFX() adding the
- * _f32 / _f64 suffix and TINY = FLT_MIN / DBL_MIN (the reference's MINVAL,
- * core/include/smolar_int.h:18,25).
+ * Included by mpdata_oracle.c with R = float / double / long, SFX() adding the
+ * _f32 / _f64 / _i64 suffix, TINY = the reference's MINVAL and R_ONE, R_HALF,
+ * R_QUAT its ONE, HALF, QUAT (core/include/smolar_int.h:12-31), R_DIV its
+ * division (C's truncating one, with a zero-divisor record, for long).
  *
  * Every expression keeps the reference's evaluation order (C's left-to-right
  * association of its macro expansions), so a strict-IEEE build reproduces
@@ -22,23 +23,23 @@ void SFX(oracle_courant)(int nx, int ny, int ns, const R* dx, const R* dy, const
     memset(U, 0, n * sizeof(R));
     memset(V, 0, n * sizeof(R));
     memset(W, 0, n * sizeof(R));
-    const R quarter_dt = (R)0.25 * dt;
+    const R quarter_dt = R_QUAT * dt;
     for (int k = 1; k < ns - 1; k++)
         for (int j = 1; j < ny - 1; j++)
             for (int i = 0; i < nx - 1; i++) {
-                R q = quarter_dt / dx[i];
+                R q = R_DIV(quarter_dt, dx[i]);
                 AT(U, i, j, k) = q * (((AT(u0, i, j, k) + AT(u0, i + 1, j, k)) +
                                        AT(u1, i, j, k)) + AT(u1, i + 1, j, k));
             }
     for (int k = 1; k < ns - 1; k++)
         for (int j = 0; j < ny - 1; j++) {
-            R q = quarter_dt / dy[j];
+            R q = R_DIV(quarter_dt, dy[j]);
             for (int i = 1; i < nx - 1; i++)
                 AT(V, i, j, k) = q * (((AT(v0, i, j, k) + AT(v0, i, j + 1, k)) +
                                        AT(v1, i, j, k)) + AT(v1, i, j + 1, k));
         }
     for (int k = 0; k < ns - 1; k++) {
-        R q = quarter_dt / ds[k];
+        R q = R_DIV(quarter_dt, ds[k]);
         for (int j = 1; j < ny - 1; j++)
             for (int i = 1; i < nx - 1; i++)
                 AT(W, i, j, k) = q * (((AT(w0, i, j, k) + AT(w0, i, j, k + 1)) +
@@ -51,13 +52,15 @@ void SFX(oracle_courant)(int nx, int ny, int ns, const R* dx, const R* dy, const
  *   ((-DIV) + (|a|(1-|a|) (c_hi - c_lo)) / ((c_hi + c_lo) + TINY))
  *     - 1/2 a ((b1 n1) / d1 + (b2 n2) / d2)
  * neg_div is -DIV on interior faces and exactly +0 on boundary faces (the
- * reference passes the integer literal 0 there). */
+ * reference passes the integer literal 0 there).  `one` is ONE for the x and
+ * y faces (uu.c:20, vv.c:23) and the literal 1 for the z faces (ww.c:22):
+ * equal except in the INTEGER build. */
 static inline R SFX(face_pattern)(R neg_div, R a, R c_lo, R c_hi,
-                                  R b1, R n1, R d1, R b2, R n2, R d2)
+                                  R b1, R n1, R d1, R b2, R n2, R d2, R one)
 {
     R ma = SFX(mag)(a);
-    R t = neg_div + ((ma * ((R)1 - ma)) * (c_hi - c_lo)) / ((c_hi + c_lo) + TINY);
-    return t - (R)0.5 * (a * (((b1 * n1) / d1) + ((b2 * n2) / d2)));
+    R t = neg_div + R_DIV((ma * (one - ma)) * (c_hi - c_lo), (c_hi + c_lo) + TINY);
+    return t - R_HALF * (a * (R_DIV(b1 * n1, d1) + R_DIV(b2 * n2, d2)));
 }
 
 /* Sum-difference pair of a transverse gradient ratio:
@@ -82,12 +85,12 @@ static void SFX(antidiff_x)(int nx, int ny, int ns, const R* c, const R* U,
                 R vb, wb, neg_div = 0;
                 if (i == 0 || i == nx - 2) {
                     int ic = (i == 0) ? 1 : nx - 2;   /* adjacent interior cell */
-                    vb = (R)0.5 * (AT(V, ic, j - 1, k) + AT(V, ic, j, k));
-                    wb = (R)0.5 * (AT(W, ic, j, k - 1) + AT(W, ic, j, k));
+                    vb = R_HALF * (AT(V, ic, j - 1, k) + AT(V, ic, j, k));
+                    wb = R_HALF * (AT(W, ic, j, k - 1) + AT(W, ic, j, k));
                 } else {
-                    vb = (R)0.25 * (((AT(V, i + 1, j - 1, k) + AT(V, i + 1, j, k)) +
+                    vb = R_QUAT * (((AT(V, i + 1, j - 1, k) + AT(V, i + 1, j, k)) +
                                      AT(V, i, j, k)) + AT(V, i, j - 1, k));
-                    wb = (R)0.25 * (((AT(W, i + 1, j, k - 1) + AT(W, i + 1, j, k)) +
+                    wb = R_QUAT * (((AT(W, i + 1, j, k - 1) + AT(W, i + 1, j, k)) +
                                      AT(W, i, j, k)) + AT(W, i, j, k - 1));
                     if (use_div) {
                         R s = AT(U, i + 1, j, k) - AT(U, i - 1, j, k);
@@ -99,7 +102,7 @@ static void SFX(antidiff_x)(int nx, int ny, int ns, const R* c, const R* U,
                         s = s - AT(W, i + 1, j, k);
                         s = s - AT(W, i, j, k);
                         s = s + AT(W, i, j, k - 1);
-                        neg_div = -(((R)0.25 * AT(U, i, j, k)) * s);
+                        neg_div = -((R_QUAT * AT(U, i, j, k)) * s);
                     } else {
                         neg_div = -(R)0;
                     }
@@ -111,7 +114,7 @@ static void SFX(antidiff_x)(int nx, int ny, int ns, const R* c, const R* U,
                           AT(c, i, j, k - 1), AT(c, i + 1, j, k - 1), n2, d2);
                 AT(Un, i, j, k) = SFX(face_pattern)(neg_div, AT(U, i, j, k),
                                                     AT(c, i, j, k), AT(c, i + 1, j, k),
-                                                    vb, n1, d1, wb, n2, d2);
+                                                    vb, n1, d1, wb, n2, d2, R_ONE);
             }
 }
 
@@ -129,8 +132,8 @@ static void SFX(antidiff_y)(int nx, int ny, int ns, const R* c, const R* U,
                 R ub, wb, neg_div = 0;
                 if (j == 0 || j == ny - 2) {
                     int jc = (j == 0) ? 1 : ny - 2;
-                    ub = (R)0.5 * (AT(U, i - 1, jc, k) + AT(U, i, jc, k));
-                    wb = (R)0.5 * (AT(W, i, jc, k - 1) + AT(W, i, jc, k));
+                    ub = R_HALF * (AT(U, i - 1, jc, k) + AT(U, i, jc, k));
+                    wb = R_HALF * (AT(W, i, jc, k - 1) + AT(W, i, jc, k));
                 } else {
                     if (i == 1 && !vv_fix) {
                         /* Never written by the reference: odd corrective passes
@@ -139,9 +142,9 @@ static void SFX(antidiff_y)(int nx, int ny, int ns, const R* c, const R* U,
                         AT(Vn, i, j, k) = (pass & 1) ? (R)0 : AT(Vadv, i, j, k);
                         continue;
                     }
-                    ub = (R)0.25 * (((AT(U, i - 1, j + 1, k) + AT(U, i, j + 1, k)) +
+                    ub = R_QUAT * (((AT(U, i - 1, j + 1, k) + AT(U, i, j + 1, k)) +
                                      AT(U, i, j, k)) + AT(U, i - 1, j, k));
-                    wb = (R)0.25 * (((AT(W, i, j + 1, k - 1) + AT(W, i, j + 1, k)) +
+                    wb = R_QUAT * (((AT(W, i, j + 1, k - 1) + AT(W, i, j + 1, k)) +
                                      AT(W, i, j, k)) + AT(W, i, j, k - 1));
                     if (use_div) {
                         R u_l2_up = (i >= 2) ? AT(U, i - 2, j + 1, k) : (R)0;
@@ -155,7 +158,7 @@ static void SFX(antidiff_y)(int nx, int ny, int ns, const R* c, const R* U,
                         s = s - u_l2_up;
                         s = s - u_l2;
                         s = s + AT(U, i - 1, j, k);
-                        neg_div = -(((R)0.25 * AT(V, i, j, k)) * s);
+                        neg_div = -((R_QUAT * AT(V, i, j, k)) * s);
                     } else {
                         neg_div = -(R)0;
                     }
@@ -167,7 +170,7 @@ static void SFX(antidiff_y)(int nx, int ny, int ns, const R* c, const R* U,
                           AT(c, i, j, k - 1), AT(c, i, j + 1, k - 1), n2, d2);
                 AT(Vn, i, j, k) = SFX(face_pattern)(neg_div, AT(V, i, j, k),
                                                     AT(c, i, j, k), AT(c, i, j + 1, k),
-                                                    ub, n1, d1, wb, n2, d2);
+                                                    ub, n1, d1, wb, n2, d2, R_ONE);
             }
 }
 
@@ -182,12 +185,12 @@ static void SFX(antidiff_z)(int nx, int ny, int ns, const R* c, const R* U,
                 R ub, vb, neg_div = 0;
                 if (k == 0 || k == ns - 2) {
                     int kc = (k == 0) ? 1 : ns - 2;
-                    ub = (R)0.5 * (AT(U, i - 1, j, kc) + AT(U, i, j, kc));
-                    vb = (R)0.5 * (AT(V, i, j - 1, kc) + AT(V, i, j, kc));
+                    ub = R_HALF * (AT(U, i - 1, j, kc) + AT(U, i, j, kc));
+                    vb = R_HALF * (AT(V, i, j - 1, kc) + AT(V, i, j, kc));
                 } else {
-                    ub = (R)0.25 * (((AT(U, i, j, k) + AT(U, i, j, k + 1)) +
+                    ub = R_QUAT * (((AT(U, i, j, k) + AT(U, i, j, k + 1)) +
                                      AT(U, i - 1, j, k + 1)) + AT(U, i - 1, j, k));
-                    vb = (R)0.25 * (((AT(V, i, j - 1, k + 1) + AT(V, i, j, k + 1)) +
+                    vb = R_QUAT * (((AT(V, i, j - 1, k + 1) + AT(V, i, j, k + 1)) +
                                      AT(V, i, j, k)) + AT(V, i, j - 1, k));
                     if (use_div) {
                         R s = AT(W, i, j, k + 1) - AT(W, i, j, k - 1);
@@ -199,7 +202,7 @@ static void SFX(antidiff_z)(int nx, int ny, int ns, const R* c, const R* U,
                         s = s - AT(V, i, j, k + 1);
                         s = s - AT(V, i, j, k);
                         s = s + AT(V, i, j - 1, k);
-                        neg_div = -(((R)0.25 * AT(W, i, j, k)) * s);
+                        neg_div = -((R_QUAT * AT(W, i, j, k)) * s);
                     } else {
                         neg_div = -(R)0;
                     }
@@ -211,7 +214,7 @@ static void SFX(antidiff_z)(int nx, int ny, int ns, const R* c, const R* U,
                           AT(c, i, j - 1, k), AT(c, i, j - 1, k + 1), n2, d2);
                 AT(Wn, i, j, k) = SFX(face_pattern)(neg_div, AT(W, i, j, k),
                                                     AT(c, i, j, k), AT(c, i, j, k + 1),
-                                                    ub, n1, d1, vb, n2, d2);
+                                                    ub, n1, d1, vb, n2, d2, (R)1);
             }
 }
 
@@ -249,7 +252,7 @@ void SFX(oracle_donor)(int nx, int ny, int ns, const R* c0, const R* U, const R*
                        SFX(upwind)(AT(c0, i, j - 1, k), cc, AT(V, i, j - 1, k));
                 R fz = SFX(upwind)(cc, AT(c0, i, j, k + 1), AT(W, i, j, k)) -
                        SFX(upwind)(AT(c0, i, j, k - 1), cc, AT(W, i, j, k - 1));
-                AT(c1, i, j, k) = cc - (R)0.5 * ((fx + fy) + fz);
+                AT(c1, i, j, k) = cc - R_HALF * ((fx + fy) + fz);
             }
 }
 
@@ -435,6 +438,7 @@ int SFX(oracle_smolar)(int nx, int ny, int ns, R* dx, R* dy, R* ds, const R dt, 
 {
     (void)flow_type; /* stored but never read by the reference (uu.c:111) */
     if (nx < 3 || ny < 3 || ns < 3 || order < 0) return -1;
+    if (R_IS_INTEGER && opts && opts->limiter) return -1; /* no limiter in the integer mode */
     R* cold = *c0;
     R* cnew = *c1;
     if (order > 0) {
@@ -443,10 +447,12 @@ int SFX(oracle_smolar)(int nx, int ny, int ns, R* dx, R* dy, R* ds, const R dt, 
         R* V = (R*)malloc(n * sizeof(R));
         R* W = (R*)malloc(n * sizeof(R));
         if (!U || !V || !W) return -1;
+        R_DIV_RESET();
         SFX(oracle_courant)(nx, ny, ns, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, U, V, W);
         int rc = SFX(pass_loop)(nx, ny, ns, U, V, W, &cold, &cnew, order, opts);
         free(U); free(V); free(W);
         if (rc) return rc;
+        if (R_DIV_FAILED()) return -2; /* a zero divisor: the reference traps there */
     }
     *c1 = cold;
     *c0 = cnew;

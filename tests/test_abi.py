@@ -75,6 +75,25 @@ def test_smolar_order_zero_only_exchanges_pointers():
     assert (c1 == 1.0).all()
 
 
+def test_smolar_i64_argument_checks_without_gpu():
+    """The INTEGER-build twin checks its arguments before any CUDA call, and
+    order 0 only exchanges the pointers, as the float entries do."""
+    import mpdata_b200 as m
+    a = _args(dtype=np.int64)
+    with pytest.raises(m.MpdataError) as e:
+        m.smolar(5, 4, 2, a["dx"], a["dy"], a["ds"][:2], 1, *([a["u"]] * 6), a["c0"], a["c1"],
+                 order=2, dtype=np.int64)
+    assert e.value.code == -1
+    with pytest.raises(m.MpdataError) as e:
+        m.smolar(5, 4, 3, a["dx"], a["dy"], a["ds"], 1, *([a["u"]] * 6), a["c0"], a["c1"],
+                 order=-1, dtype=np.int64)
+    assert e.value.code == -1
+    a["c0"][:] = 7
+    c0, c1 = m.smolar(5, 4, 3, a["dx"], a["dy"], a["ds"], 1, *([a["u"]] * 6), a["c0"], a["c1"],
+                      order=0, dtype=np.int64)
+    assert c0 is a["c1"] and c1 is a["c0"] and (c1 == 7).all()
+
+
 def test_create_rejects_bad_arguments_without_gpu():
     import mpdata_b200 as m
     for kw in (dict(nx=2, ny=5, ns=5, order=2), dict(nx=5, ny=5, ns=5, order=0)):

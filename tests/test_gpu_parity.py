@@ -40,7 +40,7 @@ def _smolar_steps(m, g, dtype, steps):
 
 
 @pytest.mark.parametrize("kernel", [0, 1], ids=["fused", "unfused"])
-@pytest.mark.parametrize("path", golden_files(), ids=os.path.basename)
+@pytest.mark.parametrize("path", golden_files(floating_only=True), ids=os.path.basename)
 def test_smolar_strict_reproduces_reference_fixtures(m, path, kernel):
     g = load_golden(path)
     m.set_default_options(m.SolverOptions(strict=True, kernel=kernel))
@@ -49,7 +49,7 @@ def test_smolar_strict_reproduces_reference_fixtures(m, path, kernel):
     assert np.array_equal(other, g["other"])
 
 
-@pytest.mark.parametrize("path", golden_files(), ids=os.path.basename)
+@pytest.mark.parametrize("path", golden_files(floating_only=True), ids=os.path.basename)
 def test_smolar_default_within_tolerance(m, path):
     g = load_golden(path)
     m.set_default_options(None)

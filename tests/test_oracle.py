@@ -86,6 +86,55 @@ def test_order_zero_exchanges_pointers(oracle_mod):
     assert rc == 0 and newest is c0 and other is c1
 
 
+# ---- the reference's INTEGER build (real = long) ----
+
+@pytest.mark.parametrize("shape,order,steps", [((17, 13, 11), 1, 3), ((9, 7, 5), 2, 2),
+                                               ((9, 7, 5), 3, 1), ((9, 7, 5), 4, 1),
+                                               ((33, 3, 6), 2, 1), ((3, 3, 3), 3, 1)])
+def test_integer_oracle_matches_reference_build(oracle_mod, shape, order, steps):
+    """Bit for bit against the reference compiled with -DINTEGER, on cases the
+    oracle first runs without a division by zero (the reference traps there)."""
+    if not oracle_mod.ref_available("i64"):
+        pytest.skip("reference INTEGER build (oracle/_ref) not present")
+    from conftest import integer_cases
+    cases = integer_cases(oracle_mod, shape, order, steps=steps, count=3)
+    assert cases, "no usable integer case"
+    for _, g, expect in cases:
+        args = (g["dx"], g["dy"], g["ds"], g["dt"], g["u0"], g["u1"], g["v0"], g["v1"],
+                g["w0"], g["w1"])
+        c0, c1 = g["c0"].copy(), np.zeros_like(g["c0"])
+        for newest_o, other_o in expect:
+            rc, newest, other = oracle_mod.ref_smolar(*args, c0, c1, order, variant="i64")
+            assert rc == 0
+            assert (newest is c1) == bool(order & 1)  # pointer exchange iff order even
+            assert np.array_equal(newest, newest_o) and np.array_equal(other, other_o)
+            c0, c1 = newest.copy(), other.copy()
+
+
+def test_integer_oracle_flags_division_by_zero(oracle_mod):
+    """The integer scheme is not positivity-preserving: some cases reach
+    c_hi + c_lo + MINVAL = 0, where the reference's division traps; the
+    oracle reports them (-2) instead of dividing."""
+    rcs = set()
+    for seed in range(40):
+        g = workloads.integer_case(9, 7, 5, seed=seed)
+        c0, c1 = g["c0"].copy(), np.zeros_like(g["c0"])
+        rc, _, _ = oracle_mod.smolar(g["dx"], g["dy"], g["ds"], g["dt"], g["u0"], g["u1"],
+                                     g["v0"], g["v1"], g["w0"], g["w1"], c0, c1, 3,
+                                     dtype=np.int64)
+        rcs.add(rc)
+    assert rcs == {0, -2}
+
+
+def test_integer_oracle_rejects_limiter(oracle_mod):
+    g = workloads.integer_case(5, 4, 3, seed=1)
+    c0, c1 = g["c0"].copy(), np.zeros_like(g["c0"])
+    rc, _, _ = oracle_mod.smolar(g["dx"], g["dy"], g["ds"], g["dt"], g["u0"], g["u1"], g["v0"],
+                                 g["v1"], g["w0"], g["w1"], c0, c1, 2, dtype=np.int64,
+                                 limiter=1)
+    assert rc == -1
+
+
 def _ring_faces(n=24, ns=10, courant=0.4):
     r = workloads.ring3d(n=n, ns=ns, courant=courant, wcourant=0.1, sigma=3.0, offset=5.0,
                          background=1e-6)
