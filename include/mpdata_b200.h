@@ -140,6 +140,9 @@ typedef struct mpdata_solver* mpdata_handle;
 /* Where a pointer argument lives. */
 #define MPDATA_HOST 0
 #define MPDATA_DEVICE 1
+/* Host memory (pinned: mpdata_host_alloc) written by a copy that is only
+ * queued: mpdata_get_planes() returns a ticket for mpdata_wait(). */
+#define MPDATA_HOST_ASYNC 2
 
 /* Divergent-flow term of the antidiffusive velocity. */
 #define MPDATA_DIV_REFERENCE 0 /* as the reference codes it (uu.c:81-84, vv.c:85-89, ww.c:88-92) */
@@ -196,11 +199,17 @@ int mpdata_get_field(mpdata_handle h, void* c, int where);
 int mpdata_get_previous(mpdata_handle h, void* c, int where);
 
 /* z-planes [k0, k0+nk) of the newest field as dense nx*ny planes (halo
- * exchange of z-slab decompositions).  get: host copies synchronise, device
- * copies are queued on the handle's stream.  set: the planes are written into
+ * exchange of z-slab decompositions, output frames).  get: host copies
+ * synchronise, device copies are queued on the handle's stream, and
+ * MPDATA_HOST_ASYNC copies are queued too and return a ticket (>= 0): the
+ * caller may step on and write out the planes after mpdata_wait(h, ticket),
+ * so frame output overlaps the next steps.  set: the planes are written into
  * every field level (planes on the grid's own z boundary are shell). */
 int mpdata_get_planes(mpdata_handle h, int k0, int nk, void* dst, int where);
 int mpdata_set_planes(mpdata_handle h, int k0, int nk, const void* src, int where);
+
+/* Wait until the MPDATA_HOST_ASYNC copy with this ticket has landed. */
+int mpdata_wait(mpdata_handle h, int ticket);
 
 /* Advance nsteps steps on the handle's stream (asynchronous). */
 int mpdata_step(mpdata_handle h, int nsteps);

@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libmpdata_b200.so")
 SOLENOIDAL, DIVERGENT = 0, 1
 MSMOLAR_SERIAL, MSMOLAR_PTHREADS, MSMOLAR_OPENMP = 0, 1, 2
 F32, F64 = 0, 1
-HOST, DEVICE = 0, 1
+HOST, DEVICE, HOST_ASYNC = 0, 1, 2
 DIV_REFERENCE, DIV_OFF = 0, 1
 
 ERRORS = {-1: "MPDATA_ERR_ARG", -2: "MPDATA_ERR_CUDA", -3: "MPDATA_ERR_NOMEM",
@@ -72,6 +72,7 @@ _lib.mpdata_step.argtypes = [_vp, C.c_int]
 _lib.mpdata_get_planes.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int]
 _lib.mpdata_set_planes.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int]
 _lib.mpdata_sync.argtypes = [_vp]
+_lib.mpdata_wait.argtypes = [_vp, C.c_int]
 _lib.mpdata_mass.argtypes = [_vp, C.POINTER(C.c_double)]
 _lib.mpdata_min.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]
 _lib.mpdata_launches_per_step.argtypes = [_vp]
@@ -344,6 +345,21 @@ class Solver:
         p, where = _ptr(out, self.dtype)
         _check(_lib.mpdata_get_planes(self._h, k0, nk, p, where))
         return out
+
+    def get_planes_async(self, k0: int, nk: int, out) -> int:
+        """Queue the copy of z-planes [k0, k0+nk) into ``out``, a C-contiguous
+        (nk, ny, nx) view of pinned host memory (``mpdata_host_alloc``), and
+        return its ticket: ``out`` holds the planes after ``wait(ticket)``
+        (``mpdata_get_planes`` with MPDATA_HOST_ASYNC)."""
+        if not (isinstance(out, np.ndarray) and out.dtype == self.dtype and out.flags.c_contiguous
+                and out.shape == (nk,) + self.shape[1:]):
+            raise TypeError("expected a C-contiguous host array of shape (nk, ny, nx)")
+        return _check(_lib.mpdata_get_planes(self._h, k0, nk, C.c_void_p(out.ctypes.data),
+                                             HOST_ASYNC))
+
+    def wait(self, ticket: int):
+        """Wait for a queued copy (``mpdata_wait``)."""
+        _check(_lib.mpdata_wait(self._h, ticket))
 
     def set_planes(self, k0: int, planes):
         """Overwrite z-planes [k0, k0+len) in every level (``mpdata_set_planes``)."""

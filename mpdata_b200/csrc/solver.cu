@@ -612,6 +612,8 @@ void free_solver(Solver* h)
         }
     for (cudaEvent_t e : h->event_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : h->pipe_ev) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->fence_ev)
+        if (e) cudaEventDestroy(e);
     if (h->s_up) cudaStreamDestroy(h->s_up);
     if (h->s_down) cudaStreamDestroy(h->s_down);
     for (int b = 0; b < 3; b++) cudaFree(h->c[b]);
@@ -905,16 +907,42 @@ int mpdata_get_planes(mpdata_handle hh, int k0, int nk, void* dst, int where)
     Solver* h = reinterpret_cast<Solver*>(hh);
     if (!h || !dst || nk < 0 || k0 < 0 || k0 + nk > (h ? h->d.ns : 0))
         return mpd::fail(MPDATA_ERR_ARG, "bad plane range");
+    if (where != MPDATA_HOST && where != MPDATA_DEVICE && where != MPDATA_HOST_ASYNC)
+        return mpd::fail(MPDATA_ERR_ARG, "bad where %d", where);
     if (!h->have_field) return mpd::fail(MPDATA_ERR_STATE, "no field set");
-    if (nk == 0) return 0;
+    if (nk == 0 && where != MPDATA_HOST_ASYNC) return 0;
     if (int rc = ensure_device(h)) return rc;
     const size_t w = (size_t)h->d.nx * h->esz;
     const char* src = (const char*)h->c[h->cur] + (size_t)k0 * h->d.pp * h->esz;
-    CUDA_TRY(cudaMemcpy2DAsync(dst, w, src, (size_t)h->d.px * h->esz, w, (size_t)h->d.ny * nk,
-                               where == MPDATA_HOST ? cudaMemcpyDeviceToHost
-                                                    : cudaMemcpyDeviceToDevice,
-                               h->stream));
-    return where == MPDATA_HOST ? mpdata_sync(hh) : 0;
+    if (nk > 0)
+        CUDA_TRY(cudaMemcpy2DAsync(dst, w, src, (size_t)h->d.px * h->esz, w,
+                                   (size_t)h->d.ny * nk,
+                                   where == MPDATA_DEVICE ? cudaMemcpyDeviceToDevice
+                                                          : cudaMemcpyDeviceToHost,
+                                   h->stream));
+    if (where == MPDATA_HOST) return mpdata_sync(hh);
+    if (where != MPDATA_HOST_ASYNC) return 0;
+    // queued host copy: fence it and hand out its ticket
+    const int slot = h->fence_n % Solver::kFences;
+    if (!h->fence_ev[slot])
+        CUDA_TRY(cudaEventCreateWithFlags(&h->fence_ev[slot], cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(h->fence_ev[slot], h->stream));
+    const int ticket = h->fence_n;
+    h->fence_n = (h->fence_n + 1) & 0x3fffffff;
+    return ticket;
+}
+
+// Wait for a queued host copy.  A ticket older than the fence ring waits on
+// the fence of a later copy, which completes after it (in stream order).
+int mpdata_wait(mpdata_handle hh, int ticket)
+{
+    Solver* h = reinterpret_cast<Solver*>(hh);
+    if (!h || ticket < 0) return mpd::fail(MPDATA_ERR_ARG, "bad ticket");
+    cudaEvent_t e = h->fence_ev[ticket % Solver::kFences];
+    if (!e) return mpd::fail(MPDATA_ERR_ARG, "no copy with ticket %d", ticket);
+    if (int rc = ensure_device(h)) return rc;
+    CUDA_TRY(cudaEventSynchronize(e));
+    return 0;
 }
 
 // Overwrite z-planes [k0, k0 + nk) in every field level (a plane on the

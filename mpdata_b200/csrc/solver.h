@@ -45,6 +45,10 @@ struct Solver {
     // Pipelined host-array step: upload and download streams, chunk events.
     cudaStream_t s_up = nullptr, s_down = nullptr;
     std::vector<cudaEvent_t> pipe_ev;
+    // Queued host copies (MPDATA_HOST_ASYNC): ticket t is fenced by fence_ev[t % kFences].
+    static constexpr int kFences = 8;
+    cudaEvent_t fence_ev[kFences] = {};
+    int fence_n = 0;  // tickets issued
     // Optional per-pass event timing: pending event pairs per pass class.
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[3];

@@ -14,7 +14,8 @@
  * Stepping: by default through the reference-compatible smolar() with host
  * arrays and the driver's pointer exchange (tests/ring2d/test.c:87-106);
  * with --device the field stays on the GPU (mpdata_step) and only the frames
- * come back.  --limiter switches the nonoscillatory option on.
+ * come back, by queued copies that overlap the next step (the whole field
+ * once, at the end).  --limiter switches the nonoscillatory option on.
  *
  * Output (headless): --frames writes, per step 0..nt, the u, v and c planes
  * of level 1 as n*n floats each (the reference's ring2d.bin layout,
@@ -158,28 +159,54 @@ int main(int argc, char** argv)
     }
     const size_t probe = (size_t)(n / 2 + n / 4) + (size_t)n * (n / 2) + n2;
     real* last = c0;
-    for (int it = 1; it <= nt; it++) {
-        real* out;
-        if (device) {
-            CHECK(mpdata_step(h, 1));
-            CHECK(mpdata_get_field(h, c1, MPDATA_HOST));
-            out = c1;
-        } else {
-            CHECK(smolar(n, n, m, dx, dy, ds, dt, u, u, v, v, w, w, &c0, &c1, DIVERGENT, order));
-            out = c1;
+    if (device) {
+        /* Frames (level 1) leave the GPU by queued copies into two pinned
+         * buffers: step it+1 and its frame copy are queued before frame it is
+         * written, so the file output overlaps the GPU's work. */
+        real* fb[2];
+        int tk[2] = {-1, -1};
+        fb[0] = (real*)mpdata_host_alloc(sizeof(real) * n2);
+        fb[1] = (real*)mpdata_host_alloc(sizeof(real) * n2);
+        if (!fb[0] || !fb[1]) return 1;
+#define QUEUE_STEP(b)                                                      \
+    do {                                                                   \
+        CHECK(mpdata_step(h, 1));                                          \
+        tk[b] = mpdata_get_planes(h, 1, 1, fb[b], MPDATA_HOST_ASYNC);      \
+        if (tk[b] < 0) {                                                   \
+            fprintf(stderr, "frame copy failed: %s\n", mpdata_last_error()); \
+            return 1;                                                      \
+        }                                                                  \
+    } while (0)
+        if (nt >= 1) QUEUE_STEP(1);
+        for (int it = 1; it <= nt; it++) {
+            const int b = it & 1;
+            if (it < nt) QUEUE_STEP(b ^ 1);
+            CHECK(mpdata_wait(h, tk[b]));
+            if (fp) {
+                fwrite(u + n2, sizeof(real), n2, fp);
+                fwrite(v + n2, sizeof(real), n2, fp);
+                fwrite(fb[b], sizeof(real), n2, fp);
+            }
+            printf("step %d %f\n", it, fb[b][probe - n2]);
         }
+#undef QUEUE_STEP
+        CHECK(mpdata_get_field(h, c1, MPDATA_HOST));
+        last = c1;
+        mpdata_host_free(fb[0]);
+        mpdata_host_free(fb[1]);
+    }
+    for (int it = 1; !device && it <= nt; it++) {
+        CHECK(smolar(n, n, m, dx, dy, ds, dt, u, u, v, v, w, w, &c0, &c1, DIVERGENT, order));
         if (fp) {
             fwrite(u + n2, sizeof(real), n2, fp);
             fwrite(v + n2, sizeof(real), n2, fp);
-            fwrite(out + n2, sizeof(real), n2, fp);
+            fwrite(c1 + n2, sizeof(real), n2, fp);
         }
-        printf("step %d %f\n", it, out[probe]);
-        last = out;
-        if (!device) {
-            real* t = c0;
-            c0 = c1;
-            c1 = t;
-        }
+        printf("step %d %f\n", it, c1[probe]);
+        last = c1;
+        real* t = c0;
+        c0 = c1;
+        c1 = t;
     }
     if (fp) fclose(fp);
     if (final_path) {

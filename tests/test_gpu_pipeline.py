@@ -65,6 +65,45 @@ def test_pipelined_smolar_same_bits(m, dtype, order, opt):
         m.set_default_options(None)
 
 
+def test_queued_plane_copies_overlap_steps(m):
+    """mpdata_get_planes(MPDATA_HOST_ASYNC) + mpdata_wait: step k+1 and its
+    plane copy are queued before the planes of step k are read (the ring
+    driver's frame output); every frame equals the synchronous copy of a
+    solver stepped alongside."""
+    g = workloads.random_case(NX, NY, NS, seed=23)
+    f = {k: (v.astype(np.float32) if isinstance(v, np.ndarray) else v) for k, v in g.items()}
+    args = (f["dx"], f["dy"], f["ds"], f["dt"], f["u0"], f["u1"], f["v0"], f["v1"], f["w0"],
+            f["w1"])
+    q, r = (m.Solver(NX, NY, NS, order=3, limiter=True) for _ in range(2))
+    for s in (q, r):
+        s.set_velocity(*args)
+        s.set_field(f["c0"])
+    lib = m.library()
+    nb = 2 * NY * NX
+    ptrs = [lib.mpdata_host_alloc(4 * nb) for _ in range(2)]
+    try:
+        buf = [np.ctypeslib.as_array((C.c_float * nb).from_address(p)).reshape(2, NY, NX)
+               for p in ptrs]
+        steps, tk = 6, [None, None]
+        q.step(1)
+        tk[1] = q.get_planes_async(1, 2, buf[1])
+        for it in range(1, steps + 1):
+            b = it & 1
+            if it < steps:
+                q.step(1)
+                tk[b ^ 1] = q.get_planes_async(1, 2, buf[b ^ 1])
+            q.wait(tk[b])
+            r.step(1)
+            assert np.array_equal(buf[b], r.get_planes(1, 2)), it
+        with pytest.raises(m.MpdataError):
+            q.wait(-1)
+    finally:
+        q.close()
+        r.close()
+        for p in ptrs:
+            lib.mpdata_host_free(C.c_void_p(p))
+
+
 def test_pipelined_smolar_pinned_buffers(m):
     """Pinned host buffers (every copy asynchronous) give the same bits."""
     g = workloads.random_case(NX, NY, NS, seed=17)
