@@ -86,6 +86,26 @@ void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W
     k_donor_v<T><<<g, dim3(32, 8), 0, s>>>(d, c0, U, V, W, c1, depth, zb, ze);
 }
 
+// Advective faces and pass 0 of planes [zb, ze) in one z march (k_courant_donor_v).
+template <typename T>
+void launch_courant_donor(const Dims& d, const T* dx, const T* dy, const T* ds, T dt,
+                          const T* u0, const T* u1, const T* v0, const T* v1, const T* w0,
+                          const T* w1, const T* c0, T* U, T* V, T* W, T* c1, int zb, int ze,
+                          cudaStream_t s)
+{
+    if (zb <= 0) zb = 1;
+    if (ze <= 0) ze = d.ns - 1;
+    if (ze <= zb) return;
+    constexpr int N = 16 / (int)sizeof(T);
+    const int gx = (int)((d.px / N + 31) / 32), gy = (d.ny - 2 + 7) / 8;
+    const long long cols = (long long)gx * gy;
+    const long long chunks = std::max(1LL, (4LL * 148 * 8 + cols - 1) / cols);
+    const int depth = std::max(4, (int)((ze - zb + chunks - 1) / chunks));
+    dim3 g(gx, gy, (ze - zb + depth - 1) / depth);
+    k_courant_donor_v<T><<<g, dim3(32, 8), 0, s>>>(d, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, c0,
+                                                    U, V, W, c1, depth, zb, ze);
+}
+
 template <typename T>
 int launch_pass_unfused(const Dims& d, const PassArgs<T>& a, T* bup, T* bdn, cudaStream_t s)
 {
@@ -111,6 +131,10 @@ int launch_pass_unfused(const Dims& d, const PassArgs<T>& a, T* bup, T* bdn, cud
                                     T*, T*, int, int, cudaStream_t);                        \
     template void launch_donor<T>(const Dims&, const T*, const T*, const T*, const T*, T*,  \
                                   int, int, int, cudaStream_t);                             \
+    template void launch_courant_donor<T>(const Dims&, const T*, const T*, const T*, T,     \
+                                          const T*, const T*, const T*, const T*, const T*, \
+                                          const T*, const T*, T*, T*, T*, T*, int, int,     \
+                                          cudaStream_t);                                    \
     template int launch_pass_unfused<T>(const Dims&, const PassArgs<T>&, T*, T*,            \
                                         cudaStream_t);                                      \
     template int launch_pass_fused<T>(const Dims&, const PassArgs<T>&, cudaStream_t);

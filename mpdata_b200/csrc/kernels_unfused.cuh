@@ -317,3 +317,112 @@ __global__ void __launch_bounds__(256) k_donor_v(Dims d, const T* __restrict__ c
         wm = w;
     }
 }
+
+// Pass 0 fused with the advective faces (R5 + R4, the per-call work of
+// smolar(): uu.c:126-138, vv.c:137-149, ww.c:143-155 then
+// smolar_pass.c:30-57).  The k_donor_v march, but the faces each cell needs
+// are formed from the cell velocities in registers and also stored for the
+// corrective passes.  Each face value is rounded on its own (explicit
+// multiply, nothing contracts it into the donor update), so faces and field
+// are the same bits as k_courant followed by k_donor_v.  Stores: U for
+// i <= nx-2, V and W for interior i (0 in the other lanes of a vector, as
+// k_courant writes), on interior rows of planes [zb, ze); the boundary faces
+// V(j = 0) by the j = 1 threads and W(k = 0) by a chunk starting at plane 1.
+// Face entries no pass reads (shell rows and planes) are left untouched.
+template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
+template <> __device__ __forceinline__ float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
+template <> __device__ __forceinline__ double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_courant_donor_v(
+    Dims d, const T* __restrict__ dx, const T* __restrict__ dy, const T* __restrict__ ds, T dt,
+    const T* __restrict__ u0, const T* __restrict__ u1, const T* __restrict__ v0,
+    const T* __restrict__ v1, const T* __restrict__ w0, const T* __restrict__ w1,
+    const T* __restrict__ c0, T* __restrict__ U, T* __restrict__ V, T* __restrict__ W,
+    T* __restrict__ c1, int depth, int zb, int ze)
+{
+    constexpr int N = Vec16<T>::N;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i0 >= d.px || j > d.ny - 2) return;
+    const int k0 = zb + (int)blockIdx.z * depth, k1 = min(ze, k0 + depth);
+    const long long Y = d.px, Z = d.pp;
+    const int nx = d.nx;
+    const T qdt = RealConst<T>::quat * dt;
+    // per-column and per-row Courant factors (QUAT dt / dx[i], uu.c:132)
+    T rx[N], rxl = T(0);
+#pragma unroll
+    for (int e = 0; e < N; e++) rx[e] = (i0 + e <= nx - 2) ? ratio<false>(qdt, dx[i0 + e]) : T(0);
+    const bool has_l = i0 >= 1 && i0 - 1 <= nx - 2;  // the face below the vector exists
+    if (has_l) rxl = ratio<false>(qdt, dx[i0 - 1]);
+    const T ry = ratio<false>(qdt, dy[j]), ryl = ratio<false>(qdt, dy[j - 1]);
+    auto in_x = [&](int e) { return i0 + e >= 1 && i0 + e <= nx - 2; };
+
+    long long q = cell(d, i0, j, k0);
+    Vec16<T> cm = ld16(c0 + q - Z), cc = ld16(c0 + q);
+    // z faces: W(k-1) from planes k-1, k; the planes k+1 are loaded per step
+    Vec16<T> wa = ld16(w0 + q - Z), wb = ld16(w1 + q - Z), wc = ld16(w0 + q), wd = ld16(w1 + q);
+    Vec16<T> wlo;
+    {
+        const T rz = ratio<false>(qdt, ds[k0 - 1]);
+#pragma unroll
+        for (int e = 0; e < N; e++)
+            wlo.v[e] = in_x(e) ? mul_rn(rz, ((wa.v[e] + wc.v[e]) + wb.v[e]) + wd.v[e]) : T(0);
+        if (k0 == 1) st16(W + q - Z, wlo);  // face plane 0
+    }
+    for (int k = k0; k < k1; k++, q += Z) {
+        const Vec16<T> cp = ld16(c0 + q + Z), cd = ld16(c0 + q - Y), cu = ld16(c0 + q + Y);
+        const T cl = __ldg(c0 + q - 1), cr = __ldg(c0 + q + N);
+        // x faces of the vector's cells and the one below its first cell
+        const Vec16<T> a0 = ld16(u0 + q), a1 = ld16(u1 + q);
+        const T a0r = __ldg(u0 + q + N), a1r = __ldg(u1 + q + N);
+        Vec16<T> uf;
+#pragma unroll
+        for (int e = 0; e < N; e++) {
+            const T r0 = e < N - 1 ? a0.v[e < N - 1 ? e + 1 : 0] : a0r;
+            const T r1 = e < N - 1 ? a1.v[e < N - 1 ? e + 1 : 0] : a1r;
+            uf.v[e] = (i0 + e <= nx - 2) ? mul_rn(rx[e], ((a0.v[e] + r0) + a1.v[e]) + r1) : T(0);
+        }
+        T ufl = T(0);
+        if (has_l)
+            ufl = mul_rn(rxl, ((__ldg(u0 + q - 1) + a0.v[0]) + __ldg(u1 + q - 1)) + a1.v[0]);
+        // y faces j+1/2 and j-1/2
+        const Vec16<T> b0 = ld16(v0 + q), b1 = ld16(v1 + q), b0u = ld16(v0 + q + Y),
+                       b1u = ld16(v1 + q + Y), b0d = ld16(v0 + q - Y), b1d = ld16(v1 + q - Y);
+        Vec16<T> vf, vfl;
+#pragma unroll
+        for (int e = 0; e < N; e++) {
+            vf.v[e] = in_x(e) ? mul_rn(ry, ((b0.v[e] + b0u.v[e]) + b1.v[e]) + b1u.v[e]) : T(0);
+            vfl.v[e] = in_x(e) ? mul_rn(ryl, ((b0d.v[e] + b0.v[e]) + b1d.v[e]) + b1.v[e]) : T(0);
+        }
+        // z face k+1/2
+        const Vec16<T> wp0 = ld16(w0 + q + Z), wp1 = ld16(w1 + q + Z);
+        const T rz = ratio<false>(qdt, ds[k]);
+        Vec16<T> wf;
+#pragma unroll
+        for (int e = 0; e < N; e++)
+            wf.v[e] = in_x(e) ? mul_rn(rz, ((wc.v[e] + wp0.v[e]) + wd.v[e]) + wp1.v[e]) : T(0);
+        st16(U + q, uf);
+        st16(V + q, vf);
+        if (j == 1) st16(V + q - Y, vfl);
+        st16(W + q, wf);
+        Vec16<T> out;
+#pragma unroll
+        for (int e = 0; e < N; e++) {
+            const int i = i0 + e;
+            const T left = e == 0 ? cl : cc.v[e > 0 ? e - 1 : 0];
+            const T right = e == N - 1 ? cr : cc.v[e < N - 1 ? e + 1 : 0];
+            const T uleft = e == 0 ? ufl : uf.v[e > 0 ? e - 1 : 0];
+            out.v[e] = (i >= 1 && i <= nx - 2)
+                           ? donor_update(cc.v[e], left, right, cd.v[e], cu.v[e], cm.v[e], cp.v[e],
+                                          uf.v[e], uleft, vf.v[e], vfl.v[e], wf.v[e], wlo.v[e])
+                           : cc.v[e];
+        }
+        st16(c1 + q, out);
+        cm = cc;
+        cc = cp;
+        wlo = wf;
+        wc = wp0;
+        wd = wp1;
+    }
+}

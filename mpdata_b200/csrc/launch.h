@@ -123,6 +123,12 @@ template <typename T> struct AdjPassArgs {
     template <typename T>                                                                  \
     void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W,      \
                       T* c1, int copy_shell, int zb, int ze, cudaStream_t s);              \
+    /* Faces of the interior rows of planes [zb, ze) and pass 0 there, one kernel. */      \
+    template <typename T>                                                                  \
+    void launch_courant_donor(const Dims& d, const T* dx, const T* dy, const T* ds, T dt,  \
+                              const T* u0, const T* u1, const T* v0, const T* v1,          \
+                              const T* w0, const T* w1, const T* c0, T* U, T* V, T* W,     \
+                              T* c1, int zb, int ze, cudaStream_t s);                      \
     /* Corrective pass, one kernel per reference routine; bup/bdn scratch (limiter). */    \
     template <typename T>                                                                  \
     int launch_pass_unfused(const Dims& d, const PassArgs<T>& a, T* bup, T* bdn,           \

@@ -237,6 +237,7 @@ int get_grid(Solver* h, void* dst, const void* src, int where)
 template <typename T> struct ModeOps {
     decltype(&mpd::fast::launch_courant<T>) courant;
     decltype(&mpd::fast::launch_donor<T>) donor;
+    decltype(&mpd::fast::launch_courant_donor<T>) courant_donor;
     decltype(&mpd::fast::launch_pass_unfused<T>) pass_unfused;
     decltype(&mpd::fast::launch_pass_fused<T>) pass_fused;
 };
@@ -245,9 +246,11 @@ template <typename T> ModeOps<T> ops(const Solver* h)
 {
     if (h->opts.strict)
         return {mpd::strict::launch_courant<T>, mpd::strict::launch_donor<T>,
-                mpd::strict::launch_pass_unfused<T>, mpd::strict::launch_pass_fused<T>};
+                mpd::strict::launch_courant_donor<T>, mpd::strict::launch_pass_unfused<T>,
+                mpd::strict::launch_pass_fused<T>};
     return {mpd::fast::launch_courant<T>, mpd::fast::launch_donor<T>,
-            mpd::fast::launch_pass_unfused<T>, mpd::fast::launch_pass_fused<T>};
+            mpd::fast::launch_courant_donor<T>, mpd::fast::launch_pass_unfused<T>,
+            mpd::fast::launch_pass_fused<T>};
 }
 
 template <typename T> int check_courant(Solver* h)
@@ -430,6 +433,11 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
     const T* dev[6];
     for (int v = 0; v < 6; v++) dev[v] = (const T*)h->vel[src_of[v]];
 
+    // the fused face+donor kernel writes only the face entries the passes read
+    if (!h->faces0_clean) {
+        for (int a = 0; a < 3; a++) CUDA_TRY(cudaMemsetAsync(h->faces[0][a], 0, fb, h->stream));
+        h->faces0_clean = true;
+    }
     // the upload stream may overwrite buffers only after earlier work on them
     CUDA_TRY(cudaEventRecord(ev_start, h->stream));
     CUDA_TRY(cudaStreamWaitEvent(h->s_up, ev_start, 0));
@@ -481,15 +489,14 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
             if (int rc = upload(i + 2)) return rc;
         if (i < NC) {
             CUDA_TRY(cudaStreamWaitEvent(h->stream, ev_up[std::min(i + 1, NC - 1)], 0));
-            op.courant(d, m, m + d.nx, m + d.nx + d.ny, (T)dt, dev[0], dev[1], dev[2], dev[3],
-                       dev[4], dev[5], F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), ul(i),
-                       uh(i) - ul(i), h->stream);
             const size_t off = (size_t)ul(i) * plane_dev, len = (size_t)(uh(i) - ul(i)) * plane_dev;
             for (int b = 1; b < 3; b++)
                 CUDA_TRY(cudaMemcpyAsync((char*)h->c[b] + off, (const char*)h->c[0] + off, len,
                                          cudaMemcpyDeviceToDevice, h->stream));
-            op.donor(d, Cb<T>(h, b0), F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), Cb<T>(h, b1), 0,
-                     cb(i), ce(i), h->stream);
+            // advective faces and pass 0 of the chunk in one march
+            op.courant_donor(d, m, m + d.nx, m + d.nx + d.ny, (T)dt, dev[0], dev[1], dev[2],
+                             dev[3], dev[4], dev[5], Cb<T>(h, b0), F<T>(h, 0, 0), F<T>(h, 0, 1),
+                             F<T>(h, 0, 2), Cb<T>(h, b1), cb(i), ce(i), h->stream);
         }
         for (int o = 1; o < P; o++) {
             const int j = i - o;
@@ -728,6 +735,7 @@ int mpd::set_velocity(Solver* h, const void* dx, const void* dy, const void* ds,
     }
     CUDA_TRY(cudaGetLastError());
     h->have_faces = true;
+    h->faces0_clean = true;  // k_courant writes every entry
     if (h->opts.check_courant)
         return h->dtype == MPDATA_F32 ? check_courant<float>(h) : check_courant<double>(h);
     return 0;
@@ -741,6 +749,7 @@ int mpd::set_faces(Solver* h, const void* U, const void* V, const void* W, int w
     for (int a = 0; a < 3; a++)
         if (int rc = put_grid(h, h->faces[0][a], src[a], where)) return rc;
     h->have_faces = true;
+    h->faces0_clean = false;
     if (h->opts.check_courant)
         return h->dtype == MPDATA_F32 ? check_courant<float>(h) : check_courant<double>(h);
     return 0;

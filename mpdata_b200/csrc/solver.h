@@ -41,6 +41,9 @@ struct Solver {
     CUtensorMap tm2_c[3];
     CUtensorMap tm2_f[3][3];
     bool have_field = false, have_faces = false;
+    // faces[0] entries no pass reads (shell rows and planes) hold 0, as
+    // k_courant writes them; set_faces may leave the caller's values there.
+    bool faces0_clean = true;
     int zdepth = 0;  // fused kernels: planes per z chunk (set by the default heuristic / autotuner)
     // Pipelined host-array step: upload and download streams, chunk events.
     cudaStream_t s_up = nullptr, s_down = nullptr;
