@@ -408,8 +408,12 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
     const int NC = (interior + D - 1) / D;
     auto cb = [&](int i) { return 1 + i * D; };
     auto ce = [&](int i) { return std::min(ns - 1, 1 + (i + 1) * D); };
-    auto ul = [&](int i) { return i == 0 ? 0 : cb(i); };        // upload / download range
-    auto uh = [&](int i) { return i == NC - 1 ? ns : ce(i); };
+    // upload range: through plane ce(i), the one the chunk's last plane reads
+    // above it, so chunk i's compute waits for its own upload only
+    auto ul = [&](int i) { return i == 0 ? 0 : ce(i - 1) + 1; };
+    auto uh = [&](int i) { return i == NC - 1 ? ns : ce(i) + 1; };
+    auto dl = [&](int i) { return i == 0 ? 0 : cb(i); };  // download range: the chunk's planes
+    auto dh = [&](int i) { return i == NC - 1 ? ns : ce(i); };
 
     if (!h->s_up) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_up, cudaStreamNonBlocking));
     if (!h->s_down) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_down, cudaStreamNonBlocking));
@@ -488,7 +492,7 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
         if (i + 2 < NC)
             if (int rc = upload(i + 2)) return rc;
         if (i < NC) {
-            CUDA_TRY(cudaStreamWaitEvent(h->stream, ev_up[std::min(i + 1, NC - 1)], 0));
+            CUDA_TRY(cudaStreamWaitEvent(h->stream, ev_up[i], 0));
             const size_t off = (size_t)ul(i) * plane_dev, len = (size_t)(uh(i) - ul(i)) * plane_dev;
             for (int b = 1; b < 3; b++)
                 CUDA_TRY(cudaMemcpyAsync((char*)h->c[b] + off, (const char*)h->c[0] + off, len,
@@ -511,8 +515,8 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
         if (j >= 0 && j < NC) {
             CUDA_TRY(cudaEventRecord(ev_done[j], h->stream));
             CUDA_TRY(cudaStreamWaitEvent(h->s_down, ev_done[j], 0));
-            if (int rc = down(newest, h->c[cur], ul(j), uh(j))) return rc;
-            if (int rc = down(prev, h->c[prv], ul(j), uh(j))) return rc;
+            if (int rc = down(newest, h->c[cur], dl(j), dh(j))) return rc;
+            if (int rc = down(prev, h->c[prv], dl(j), dh(j))) return rc;
         }
     }
     CUDA_TRY(cudaGetLastError());
