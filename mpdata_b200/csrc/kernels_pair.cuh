@@ -598,11 +598,19 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
             const float2 bu2 = ld2(sBU + PK * WPL + p.w), bd2 = ld2(sBD + PK * WPL + p.w);
             float2 lu = ru_prev, lv = rv_prev;
             lu.x = limit(ru_prev.x, bu.x, bd.x, bu.y, bd.y);
-            if (!edge_x) lu.y = limit(ru_prev.y, bu.y, bd.y, bu1[p.w + 2], bd1[p.w + 2]);
-            if (!edge_y) {
+            // The edge threads' outer faces (x = 31|32, y = CY-1|CY) have no ratio on
+            // the far side in this CTA and stay raw (no kept cell uses them); both
+            // forms are evaluated and selected, without a divergent branch (the far
+            // reads stay inside shared memory: x + 2 <= 33 < WX, and row CY + 1 of
+            // a ratio plane is the first row of the next work array).
+            {
+                const float buR = bu1[p.w + 2], bdR = bd1[p.w + 2];
                 const float2 buU = ld2(bu1 + p.w + WX), bdU = ld2(bd1 + p.w + WX);
-                lv = make_float2(limit(rv_prev.x, bu.x, bd.x, buU.x, bdU.x),
-                                 limit(rv_prev.y, bu.y, bd.y, buU.y, bdU.y));
+                const float luy = limit(ru_prev.y, bu.y, bd.y, buR, bdR);
+                const float2 lvl = make_float2(limit(rv_prev.x, bu.x, bd.x, buU.x, bdU.x),
+                                               limit(rv_prev.y, bu.y, bd.y, buU.y, bdU.y));
+                lu.y = edge_x ? ru_prev.y : luy;
+                lv = edge_y ? rv_prev : lvl;
             }
             const float2 lw = make_float2(limit(rw_pp.x, bu2.x, bd2.x, bu.x, bd.x),
                                           limit(rw_pp.y, bu2.y, bd2.y, bu.y, bd.y));
@@ -704,24 +712,16 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 // bounds over the cell and its face neighbours (z only in 3D)
                 const float* cnS = slot(S, 4);
                 const float mAB = fmaxf(mx0.x, mx0.y), nAB = fminf(mn0.x, mn0.y);
-                float mR, nR;
-                if (edge_x) {
-                    const float cnR = cnS[p.o + 2];
-                    mR = fmaxf(c2, cnR);
-                    nR = fminf(c2, cnR);
-                } else {
-                    mR = sMX[p.w + 2];
-                    nR = sMN[p.w + 2];
-                }
-                float2 mU, nU;
-                if (edge_y) {
-                    const float2 cnU = ld2(cnS + p.o + Y);
-                    mU = max2(cU, cnU);
-                    nU = min2(cU, cnU);
-                } else {
-                    mU = ld2(sMX + p.w + WX);
-                    nU = ld2(sMN + p.w + WX);
-                }
+                // edge threads: the neighbour's extrema from the staged planes;
+                // both forms evaluated and selected (no divergent branch)
+                const float cnR = cnS[p.o + 2];
+                const float2 cnU = ld2(cnS + p.o + Y);
+                const float mRs = sMX[p.w + 2], nRs = sMN[p.w + 2];
+                const float2 mUs = ld2(sMX + p.w + WX), nUs = ld2(sMN + p.w + WX);
+                const float mR = edge_x ? fmaxf(c2, cnR) : mRs;
+                const float nR = edge_x ? fminf(c2, cnR) : nRs;
+                const float2 mU = edge_y ? max2(cU, cnU) : mUs;
+                const float2 nU = edge_y ? min2(cU, cnU) : nUs;
                 float2 mx = make_float2(fmaxf(mAB, sMX[p.w - 1]), fmaxf(mAB, mR));
                 float2 mn = make_float2(fminf(nAB, sMN[p.w - 1]), fminf(nAB, nR));
                 mx = max2(mx, max2(ld2(sMX + p.w - WX), mU));
