@@ -358,6 +358,12 @@ __device__ __forceinline__ void store_pair(float* out, float2 v, bool a, bool b)
     else if (a) out[0] = v.x;
     else if (b) out[1] = v.y;
 }
+// Each owned lane as its own predicated scalar store (no branch).
+__device__ __forceinline__ void store_lanes(float* out, float2 v, bool a, bool b)
+{
+    if (a) out[0] = v.x;
+    if (b) out[1] = v.y;
+}
 // The same with a tile-edge pair's one owned lane as a single scalar store of
 // the selected lane (measured faster in the march without the limiter,
 // slower in the one with it).
@@ -643,7 +649,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 // face-plane k-2: the high face of plane k-2, and face-plane 0 only in
                 // the chunk that starts at plane 1 (a later chunk's warm-up does not form it)
                 if (k >= 2 && k - 2 < z1 && (k - 2 >= z0 || (k - 2 == 0 && z0 == 1)))
-                    store_pair(a.Wn + (q1 - pp), lw, p.ownA, p.ownB);
+                    store_lanes(a.Wn + (q1 - pp), lw, p.ownA, p.ownB);
             }
             const int u = k - 2;
             if (u >= z0 && u < z1 && (p.ownA || p.ownB)) {
@@ -652,8 +658,8 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 const float2 dxo = ld2(dxp + p.w);
                 const float2 netx = make_float2(dxo.x - dxp[p.w - 1], dxo.y - dxo.x);
                 const float2 nety = ld2(dyp + p.w) - ld2(dyp + p.w - WX);
-                store_pair(a.c_out + (q1 - pp), cq0 - ((netx + nety) + (dz - dz_prev)), p.ownA,
-                           p.ownB);
+                store_lanes(a.c_out + (q1 - pp), cq0 - ((netx + nety) + (dz - dz_prev)), p.ownA,
+                            p.ownB);
             }
             dz_prev = dz;
         }
