@@ -351,26 +351,13 @@ __device__ __forceinline__ PairSetup pair_setup(const Dims& d, const PassArgs<fl
     return p;
 }
 
-// Store the lanes of a pair this CTA owns (both: one 8-byte store).
-__device__ __forceinline__ void store_pair(float* out, float2 v, bool a, bool b)
-{
-    if (a && b) pair::st2(out, v);
-    else if (a) out[0] = v.x;
-    else if (b) out[1] = v.y;
-}
-// Each owned lane as its own predicated scalar store (no branch).
+// Store the lanes of a pair this CTA owns, each as its own predicated scalar
+// store.  Measured faster than one 8-byte store behind a branch on ownership
+// (tile-edge pairs own one lane, so that branch diverges).
 __device__ __forceinline__ void store_lanes(float* out, float2 v, bool a, bool b)
 {
     if (a) out[0] = v.x;
     if (b) out[1] = v.y;
-}
-// The same with a tile-edge pair's one owned lane as a single scalar store of
-// the selected lane (measured faster in the march without the limiter,
-// slower in the one with it).
-__device__ __forceinline__ void store_pair_sel(float* out, float2 v, bool a, bool b)
-{
-    if (a && b) pair::st2(out, v);
-    else if (a || b) out[b ? 1 : 0] = b ? v.y : v.x;
 }
 
 // ---- without the limiter: faces of plane k -> sync -> update of plane k ----
@@ -472,18 +459,17 @@ __device__ __forceinline__ void pair_march_plain(const Dims& d, const PassArgs<f
             {  // every thread forms its pair's update; owned lanes are stored
                 const float2 netx = make_float2(dx.x - sDX[p.w - 1], dx.y - dx.x);
                 const float2 nety = dy - ld2(sDY + p.w - WX);
-                store_pair_sel(a.c_out + q, cq2 - ((netx + nety) + (dz - dz_prev)), p.ownA,
-                               p.ownB);
+                store_lanes(a.c_out + q, cq2 - ((netx + nety) + (dz - dz_prev)), p.ownA, p.ownB);
             }
             if (a.write_faces) {
                 if (p.wxA) a.Un[q] = ru.x;
                 if (p.wxB) a.Un[q + 1] = ru.y;
                 if (p.wyA) a.Vn[q] = rv.x;
                 if (p.wyB) a.Vn[q + 1] = rv.y;
-                store_pair_sel(a.Wn + q, rw, p.ownA, p.ownB);
+                store_lanes(a.Wn + q, rw, p.ownA, p.ownB);
             }
         } else if (k == 0 && z0 == 1 && a.write_faces) {  // face-plane 0 (below plane 1)
-            store_pair_sel(a.Wn + p.col, rw, p.ownA, p.ownB);
+            store_lanes(a.Wn + p.col, rw, p.ownA, p.ownB);
         }
         dz_prev = dz;
         cq1 = cq2;
