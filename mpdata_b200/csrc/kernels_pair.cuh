@@ -638,7 +638,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                     store_lanes(a.Wn + (q1 - pp), lw, p.ownA, p.ownB);
             }
             const int u = k - 2;
-            if (u >= z0 && u < z1 && (p.ownA || p.ownB)) {
+            if (u >= z0 && u < z1) {  // uniform; every thread forms its pair's update
                 const float* dxp = sDX + PK * WPL;  // donor fluxes of plane k-2
                 const float* dyp = sDY + PK * WPL;
                 const float2 dxo = ld2(dxp + p.w);
