@@ -63,6 +63,11 @@ struct mpdata_adjoint {
     void* zblock = nullptr;
     size_t zblock_bytes = 0, zRB_bytes = 0;
     bool have_faces = false;
+    // A full segment of the backward sweep (replay + adjoint steps) as a CUDA
+    // graph, captured on first use; one per parity of the adjoint buffers at
+    // the segment's start (an odd interval swaps them segment by segment).
+    cudaGraphExec_t seg_graph[2] = {nullptr, nullptr};
+    cudaStream_t cap_stream = nullptr;  // private stream the capture records on
 };
 
 namespace {
@@ -224,19 +229,61 @@ template <typename T> int backward_impl(mpdata_adjoint* h, const void* lamN, voi
     T* lam_b = (T*)h->lam_lev[P + 1];  // adjoint of its input
     if (int rc = put(h, lam_a, lamN, where)) return rc;
     const int nseg = (N + h->every - 1) / h->every;
-    for (int seg = nseg - 1; seg >= 0; seg--) {
-        const int len = std::min(h->every, N - seg * h->every);
-        // recompute the segment from its checkpoint, keeping every intermediate
-        CUDA_TRY(cudaMemcpyAsync(h->rec[0].lev[0], h->ckpt[seg], fb, cudaMemcpyDeviceToDevice, h->stream));
+    // recompute a segment from its checkpoint (staged in rec[0].lev[0]),
+    // keeping every intermediate, then apply its adjoint, last step first
+    auto segment = [&](int len) -> int {
         for (int t = 0; t < len; t++) {
             T* out = (t + 1 < len) ? (T*)h->rec[t + 1].lev[0] : (T*)h->tmp[0];
             step_fwd<T>(h, (const T*)h->rec[t].lev[0], out, &h->rec[t]);
         }
-        // then its adjoint, last step first
         for (int t = len - 1; t >= 0; t--) {
             if (int rc = step_adj<T>(h, h->rec[t], lam_a, lam_b)) return rc;
             std::swap(lam_a, lam_b);
         }
+        return 0;
+    };
+    for (int seg = nseg - 1; seg >= 0; seg--) {
+        const int len = std::min(h->every, N - seg * h->every);
+        CUDA_TRY(cudaMemcpyAsync(h->rec[0].lev[0], h->ckpt[seg], fb, cudaMemcpyDeviceToDevice, h->stream));
+        if (len < h->every) {  // a short last segment: launched directly
+            if (int rc = segment(len)) return rc;
+            continue;
+        }
+        // full segments: the same launches on the same buffers every time,
+        // replayed from one captured graph (hundreds of launches -> one)
+        const int par = (lam_a == (T*)h->lam_lev[P]) ? 0 : 1;
+        if (!h->seg_graph[par]) {
+            // recorded on a private stream (the caller's may be the legacy
+            // default stream, which cannot be captured), launched on the caller's
+            if (!h->cap_stream)
+                CUDA_TRY(cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking));
+            cudaStream_t user = h->stream;
+            h->stream = h->cap_stream;
+            cudaError_t eb = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+            if (eb != cudaSuccess) {
+                h->stream = user;
+                return mpd::fail(MPDATA_ERR_CUDA, "segment capture: %s", cudaGetErrorString(eb));
+            }
+            const int rc = segment(len);  // swaps lam_a / lam_b as the graph will
+            cudaGraph_t g = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(h->stream, &g);
+            h->stream = user;
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (ec != cudaSuccess)
+                return mpd::fail(MPDATA_ERR_CUDA, "segment capture: %s", cudaGetErrorString(ec));
+            const cudaError_t ei = cudaGraphInstantiate(&h->seg_graph[par], g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) {
+                h->seg_graph[par] = nullptr;
+                return mpd::fail(MPDATA_ERR_CUDA, "segment graph: %s", cudaGetErrorString(ei));
+            }
+        } else if (len & 1) {
+            std::swap(lam_a, lam_b);
+        }
+        CUDA_TRY(cudaGraphLaunch(h->seg_graph[par], h->stream));
     }
     if (int rc = get(h, lam0, lam_a, where)) return rc;
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -248,6 +295,9 @@ void destroy(mpdata_adjoint* h)
 {
     if (!h) return;
     cudaStreamSynchronize(h->stream);
+    for (cudaGraphExec_t g : h->seg_graph)
+        if (g) cudaGraphExecDestroy(g);
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     for (void* p : h->blocks) cudaFree(p);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
     delete h;
