@@ -100,6 +100,27 @@ __device__ __forceinline__ T face_v2(const Nb2<T>& n, int i, int j, int ny, int 
     return t - T(0.5) * (n.v * ratio<AP>(ub * n1, d1));
 }
 
+// Asynchronous 4- or 8-byte copy global -> shared (cp.async, bypassing
+// registers); n_src = 0 copies nothing and fills the element with zeros.
+template <typename T>
+__device__ __forceinline__ void cp_async_el(T* dst, const T* src, bool valid)
+{
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(s), "l"(src),
+                     "r"(valid ? 4 : 0)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(src),
+                     "r"(valid ? 8 : 0)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 }  // namespace ens
 
 // Donor-cell pass (smolar_pass.c:30-57, 2D), one thread per cell of a tile.
@@ -110,7 +131,7 @@ __global__ void __launch_bounds__(TX * TY)
 {
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
         const EnsItem item = items[it];
-        const EnsInst in = insts[item.inst];
+        const EnsInst& in = insts[item.inst];  // fields read in place (no local copy)
         const int i = item.i0 + threadIdx.x, j = item.j0 + threadIdx.y;
         if (i > in.nx - 2 || j > in.ny - 2) continue;
         const long long q = (long long)j * in.px + i;
@@ -135,35 +156,56 @@ __global__ void __launch_bounds__(TX * TY)
     constexpr int NT = TX * TY;
     constexpr int OW = LIM ? 1 : 0;
     constexpr int WX = TX + 2, WPL = WX * (TY + 2);  // work planes: local [-1, TX] x [-1, TY]
-    __shared__ T sC[PL], sU[PL], sV[PL], sN[LIM ? PL : 1];
+    // Stage buffers, double-buffered: the next item's tile is copied in
+    // (cp.async) while the current one is computed.
+    __shared__ T bC[2][PL], bU[2][PL], bV[2][PL], bN[2][LIM ? PL : 1];
     __shared__ T sRU[WPL], sRV[WPL], sBU[LIM ? WPL : 1], sBD[LIM ? WPL : 1];
     const int x = threadIdx.x, y = threadIdx.y, tid = y * TX + x;
     const int o = (y + H) * SX + (x + H);
     const int w = (y + 1) * WX + (x + 1);
     const bool ex_u = tid < TY, ex_v = tid >= TY && tid < TY + TX;
 
-    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    // Queue the copies of item `it`'s tile (cells outside the instance read 0).
+    auto stage = [&](int it, int b) {
         const EnsItem item = items[it];
-        const EnsInst in = insts[item.inst];
-        const int nx = in.nx, ny = in.ny, px = in.px;
-        const int i0 = item.i0 - OW, j0 = item.j0 - OW;  // global cell of local (0, 0)
+        const EnsInst& in = insts[item.inst];  // fields read in place (no local copy)
+        const int i0 = item.i0 - OW, j0 = item.j0 - OW;
         const T* gc = arena + in.c[p.in];
         const T* gn = arena + in.c[p.cn];
         const T* gu = arena + in.f[p.rs][0];
         const T* gv = arena + in.f[p.rs][1];
-        const T* vadv = arena + in.f[0][1];
-        __syncthreads();  // the previous item's reads of the stage are done
         for (int e = tid; e < PL; e += NT) {
             const int sy = e / SX, sx = e - sy * SX;
             const int gi = i0 - H + sx, gj = j0 - H + sy;
-            const bool inside = gi >= 0 && gi < nx && gj >= 0 && gj < ny;
-            const long long q = (long long)gj * px + gi;
-            sC[e] = inside ? gc[q] : T(0);
-            sU[e] = inside ? gu[q] : T(0);
-            sV[e] = inside ? gv[q] : T(0);
-            if (LIM) sN[e] = inside ? gn[q] : T(0);
+            const bool inside = gi >= 0 && gi < in.nx && gj >= 0 && gj < in.ny;
+            const long long q = inside ? (long long)gj * in.px + gi : 0;
+            cp_async_el(&bC[b][e], gc + q, inside);
+            cp_async_el(&bU[b][e], gu + q, inside);
+            cp_async_el(&bV[b][e], gv + q, inside);
+            if (LIM) cp_async_el(&bN[b][e], gn + q, inside);
         }
-        __syncthreads();
+        cp_async_commit();
+    };
+
+    int b = 0;
+    if ((int)blockIdx.x < nitems) stage(blockIdx.x, 0);
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x, b ^= 1) {
+        if (it + (int)gridDim.x < nitems) {  // the next item's tile into the other buffer
+            stage(it + gridDim.x, b ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();  // this item's tile has landed for every thread
+        const T* sC = bC[b];
+        const T* sU = bU[b];
+        const T* sV = bV[b];
+        const T* sN = bN[b];
+        const EnsItem item = items[it];
+        const EnsInst& in = insts[item.inst];  // fields read in place (no local copy)
+        const int nx = in.nx, ny = in.ny, px = in.px;
+        const int i0 = item.i0 - OW, j0 = item.j0 - OW;  // global cell of local (0, 0)
+        const T* vadv = arena + in.f[0][1];
 
         const int i = i0 + x, j = j0 + y;
         const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
@@ -239,6 +281,7 @@ __global__ void __launch_bounds__(TX * TY)
                 if (j == 1) arena[in.f[p.ws][1] + q - px] = vb;
             }
         }
+        __syncthreads();  // every read of this buffer is done before it is refilled
     }
 }
 
