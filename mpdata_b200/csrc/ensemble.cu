@@ -72,8 +72,10 @@ int build_items(mpdata_ensemble* e)
 {
     for (int t = 0; t < kTiles; t++)
         for (int kind = 0; kind < 2; kind++) {
-            const int ow = (kind == 1 && e->opts.limiter) ? 1 : 0;
-            const int sx = kTileX[t] - 2 * ow, sy = kTileY[t] - 2 * ow;
+            // cells a pass item owns: the tile less 2 low + 1 high halo cells
+            // with the limiter, 1 low without (k_ens_pass LO / HI); donor: all
+            const int halo = kind == 0 ? 0 : (e->opts.limiter ? 3 : 1);
+            const int sx = kTileX[t] - halo, sy = kTileY[t] - halo;
             std::vector<mpd::EnsItem> v;
             for (int q = 0; q < e->n; q++)
                 for (int j0 = 1; j0 <= e->ny[q] - 2; j0 += sy)

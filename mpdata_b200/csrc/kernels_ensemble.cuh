@@ -154,7 +154,10 @@ __global__ void __launch_bounds__(TX * TY)
     using namespace ens;
     constexpr int SX = TX + 2 * H, SY = TY + 2 * H, PL = SX * SY;
     constexpr int NT = TX * TY;
-    constexpr int OW = LIM ? 1 : 0;
+    // Owned cells: local x in [LO, TX-1-HI] (likewise y).  The halo cells are
+    // the ones whose high faces (and, with the limiter, ratios) the owned
+    // cells read, so every face needed is formed by a thread of the tile.
+    constexpr int LO = LIM ? 2 : 1, HI = LIM ? 1 : 0;
     constexpr int WX = TX + 2, WPL = WX * (TY + 2);  // work planes: local [-1, TX] x [-1, TY]
     // Stage buffers, double-buffered: the next item's tile is copied in
     // (cp.async) while the current one is computed.
@@ -163,13 +166,12 @@ __global__ void __launch_bounds__(TX * TY)
     const int x = threadIdx.x, y = threadIdx.y, tid = y * TX + x;
     const int o = (y + H) * SX + (x + H);
     const int w = (y + 1) * WX + (x + 1);
-    const bool ex_u = tid < TY, ex_v = tid >= TY && tid < TY + TX;
 
     // Queue the copies of item `it`'s tile (cells outside the instance read 0).
     auto stage = [&](int it, int b) {
         const EnsItem item = items[it];
         const EnsInst& in = insts[item.inst];  // fields read in place (no local copy)
-        const int i0 = item.i0 - OW, j0 = item.j0 - OW;
+        const int i0 = item.i0 - LO, j0 = item.j0 - LO;
         const T* gc = arena + in.c[p.in];
         const T* gn = arena + in.c[p.cn];
         const T* gu = arena + in.f[p.rs][0];
@@ -204,12 +206,12 @@ __global__ void __launch_bounds__(TX * TY)
         const EnsItem item = items[it];
         const EnsInst& in = insts[item.inst];  // fields read in place (no local copy)
         const int nx = in.nx, ny = in.ny, px = in.px;
-        const int i0 = item.i0 - OW, j0 = item.j0 - OW;  // global cell of local (0, 0)
+        const int i0 = item.i0 - LO, j0 = item.j0 - LO;  // global cell of local (0, 0)
         const T* vadv = arena + in.f[0][1];
 
         const int i = i0 + x, j = j0 + y;
         const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
-        const bool owned = cell_in && (!LIM || (x >= 1 && x <= TX - 2 && y >= 1 && y <= TY - 2));
+        const bool owned = cell_in && x >= LO && x <= TX - 1 - HI && y >= LO && y <= TY - 1 - HI;
         T ru = T(0), rv = T(0);
         {
             const Nb2<T> nb = gather2(sC, sU, sV, o, SX);
@@ -221,21 +223,6 @@ __global__ void __launch_bounds__(TX * TY)
         }
         sRU[w] = ru;
         sRV[w] = rv;
-        if (ex_u || ex_v) {  // faces just below the tile
-            const int ei = ex_u ? i0 - 1 : i0 + (tid - TY);
-            const int ej = ex_u ? j0 + tid : j0 - 1;
-            const int eo = (ej - j0 + H) * SX + (ei - i0 + H);
-            T ev = T(0);
-            const Nb2<T> nb = gather2(sC, sU, sV, eo, SX);
-            if (ex_u && ei >= 0 && ei <= nx - 2 && ej >= 1 && ej <= ny - 2)
-                ev = face_u2<AP>(nb, ei, nx, p.use_div);
-            if (ex_v && ei >= 1 && ei <= nx - 2 && ej >= 0 && ej <= ny - 2) {
-                const T va = (ei == 1) ? vadv[(long long)ej * px + 1] : T(0);
-                ev = face_v2<AP>(nb, ei, ej, ny, p.use_div, p.vv_fix, p.pass, va);
-            }
-            if (ex_u) sRU[(tid + 1) * WX] = ev;
-            else sRV[tid - TY + 1] = ev;
-        }
         __syncthreads();
 
         T ur = ru, ul = sRU[w - 1], vt = rv, vb = sRV[w - WX];
