@@ -256,13 +256,17 @@ __global__ void __launch_bounds__(fused::NT, sizeof(T) == 4 ? 2 : 1)
     const bool owned = cell_in && (!LIM || (x >= 1 && x <= BX - 2 && y >= 1 && y <= BY - 2));
     const bool u_ok = i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2;  // own x face exists
     const bool v_ok = i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2;  // own y face exists
-    // Extra faces below the column: threads 0..BY-1 the x faces at local x = -1,
-    // threads BY..BY+BX-1 the y faces at local y = -1.
-    const bool ex_u = tid < BY, ex_v = tid >= BY && tid < BY + BX;
-    const int ex_i = ex_u ? i0 - 1 : i0 + (tid - BY);
-    const int ex_j = ex_u ? j0 + tid : j0 - 1;
-    const int ex_o = ex_u ? (tid + 2) * Y + (1 + rx) : Y + (tid - BY + 2 + rx);
-    const int ex_w = ex_u ? (tid + 1) * WX : (tid - BY + 1);
+    // Extra faces below the column: the x faces at local x = -1 by half of warp
+    // 2, the y faces at local y = -1 by warp 3, so no warp runs both face
+    // paths one after the other (measured faster than warps 0-1 doing both).
+    constexpr int EXU0 = 2 * 32, EXV0 = 3 * 32;
+    static_assert(EXU0 + BY <= EXV0 && EXV0 + BX <= NT, "extra-face threads out of the CTA");
+    const int tu = tid - EXU0, tv = tid - EXV0;  // index along the tile's low edge
+    const bool ex_u = tu >= 0 && tu < BY, ex_v = tv >= 0 && tv < BX;
+    const int ex_i = ex_u ? i0 - 1 : i0 + tv;
+    const int ex_j = ex_u ? j0 + tu : j0 - 1;
+    const int ex_o = ex_u ? (tu + 2) * Y + (1 + rx) : Y + (tv + 2 + rx);
+    const int ex_w = ex_u ? (tu + 1) * WX : (tv + 1);
     const bool ex_ok = ex_u ? (ex_i >= 0 && ex_i <= nx - 2 && ex_j >= 1 && ex_j <= ny - 2)
                             : (ex_v && ex_i >= 1 && ex_i <= nx - 2 && ex_j >= 0 && ex_j <= ny - 2);
 
