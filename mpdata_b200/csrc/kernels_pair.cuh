@@ -24,17 +24,19 @@
 //    (clamped to <= 1) and the donor fluxes F = a (a > 0 ? c_lo : c_hi),
 //    so the donor update needs no neighbour c values.
 //  * No extra low faces are formed: the CTA's cells overlap their
-//    neighbours' (x: cell 0,1 and 31, y: row 0 and 31 with the limiter;
-//    x: 0 and 31, y: 0 without), so every face a kept cell needs is the high
-//    face of a cell of the same CTA.
+//    neighbours' (with the limiter x 0..2 and 31, rows 0, 1 and CY-1 are not
+//    updated; without it x 0 and 31 and row 0), so every face a kept cell
+//    needs is the high face of a cell of the same CTA.
+//  * No divergent branches in the plane body: tile-edge threads select, and
+//    owned lanes are written by predicated scalar stores.
 //
-// Per plane k (limiter): raw faces of plane k and z face k+1/2 -> sync ->
-// ratios of plane k -> sync -> limited x/y faces of plane k, limited z face
-// k-1/2, donor fluxes -> donor update of plane k-1.  Without the limiter the
+// Per plane k (limiter): [limited x/y faces of plane k-1, limited z face
+// k-3/2, donor fluxes, update of plane k-2; raw faces of plane k and z face
+// k+1/2] -> sync -> [ratios of plane k] -> sync.  Without the limiter the
 // update of plane k follows the raw faces after one sync.
 //
-// The step input c^n (limiter bounds) is read with one 64-bit global load
-// per pair and plane, one plane ahead.  Every wait is bounded (tma.cuh).
+// The planes of c, the previous faces and (with the limiter) the step input
+// c^n are staged by TMA, four planes deep.  Every wait is bounded (tma.cuh).
 //
 // Included by kernels_pair.cu inside namespace mpd::fast.
 
