@@ -7,9 +7,10 @@
 // and, with the limiter, the cell's in/out ratios; then it applies the
 // donor-cell update.  Without the limiter every cell of the CTA is updated;
 // with it the outer ring of the CTA is a halo (30 x 14 cells updated) whose
-// faces and ratios the limited faces of the updated cells need.  The first
-// warps also form the faces just below the column (x face at local x = -1, y
-// face at local y = -1), which the lowest cells read.
+// faces and ratios the limited faces of the updated cells need.  Warps 2 and
+// 3 also form the faces just below the column (x faces at local x = -1 by
+// half of warp 2, y faces at local y = -1 by warp 3), which the lowest cells
+// read.
 //
 // Staging.  The pass input c, the step input c^n (limiter bounds) and the
 // previous pass's faces U, V, W are brought in one plane at a time by TMA
