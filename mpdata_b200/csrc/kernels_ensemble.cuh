@@ -8,11 +8,14 @@
 // otherwise) give the same values as the 3D kernels on the 3-plane form.
 //
 // Work list: (instance, tile) items over the instances' interior cells.  A
-// persistent grid of CTAs walks the list (item = blockIdx.x + n * gridDim.x);
-// per item the CTA stages the tile with a halo of 3 into shared memory with
-// coalesced loads, forms the faces (and, with the limiter, the ratios of the
-// tile plus a one-cell ring), and updates its cells.  Tile shape TX x TY is a
-// template parameter chosen by the host-side autotuner.
+// persistent grid of CTAs walks the list (item = blockIdx.x + n * gridDim.x).
+// The corrective pass stages each item's tile with a halo of 3 into shared
+// memory by cp.async, double-buffered (the next item's copies run while the
+// current item computes), forms the faces of every cell of the tile (and,
+// with the limiter, their ratios) and updates the cells it owns: all but the
+// first column and row (the first two and the last with the limiter), so
+// every face an owned cell reads is the high face of a tile cell.  Tile shape
+// TX x TY is a template parameter chosen by the host-side autotuner.
 //
 // Included by kernels_all.cuh inside namespace mpd::MPD_NS.
 
