@@ -6,7 +6,9 @@
 // intermediate kept (levels, raw and limited faces, limiter ratios), then the
 // adjoint of each step is applied in reverse (kernels_adjoint.cuh), pass by
 // pass, last pass first.  Memory: N/every checkpoints + one segment of step
-// records, so long windows fit in HBM.
+// records, so long windows fit in HBM.  A full segment's launches (replay and
+// reverse steps, on fixed buffers) are captured once as a CUDA graph and
+// replayed for every full segment.
 //
 // The faces are steady (set once); the adjoint is with respect to the field.
 #include <cuda_runtime.h>

@@ -5,7 +5,9 @@
 //   * three field buffers rotate so the step's input c^n stays intact for the
 //     limiter bounds while passes ping-pong between the other two;
 //   * the advective faces are computed once per velocity update (the
-//     reference recomputes them on every call, smolar.c:40-42);
+//     reference recomputes them on every call, smolar.c:40-42); the
+//     pipelined host-array step behind smolar() forms them per call, fused
+//     with pass 0 chunk by chunk, overlapping the uploads and downloads;
 //   * pseudo-velocities are Jacobi-updated between two face sets
 //     (pvelocity.c:22-36), the advective set staying untouched;
 //   * the fixed boundary shell is written into all three buffers once, when
