@@ -123,7 +123,7 @@ __global__ void k_stats_final(const double* __restrict__ part, int nblk, double*
     out[2] = N;
 }
 
-// max |face| over the used entries of the three face arrays.
+// max |face| over the three face arrays, whole (unused entries hold 0).
 template <typename T>
 __global__ void k_facemax(Dims d, const T* __restrict__ U, const T* __restrict__ V,
                           const T* __restrict__ W, double* __restrict__ part)
