@@ -97,6 +97,10 @@ def test_queued_plane_copies_overlap_steps(m):
             assert np.array_equal(buf[b], r.get_planes(1, 2)), it
         with pytest.raises(m.MpdataError):
             q.wait(-1)
+        # an unknown destination kind is an argument error, not a copy
+        out = np.zeros((2, NY, NX), np.float32)
+        rc = m.library().mpdata_get_planes(q._h, 1, 2, C.c_void_p(out.ctypes.data), 7)
+        assert rc == -1 and not out.any()
     finally:
         q.close()
         r.close()
