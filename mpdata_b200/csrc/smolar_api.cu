@@ -218,6 +218,7 @@ int decomp_create(Decomp** out, int nx, int ny, int ns, T* dx, T* dy, T* ds, T d
     Solver* g = D->global;
     const void* vel[6] = {u0, u1, v0, v1, w0, w1};
     if (int rc = mpd::set_velocity(g, dx, dy, ds, (double)dt, vel, MPDATA_HOST)) return rc;
+    if (int rc = mpd::materialize_faces(g)) return rc;  // the blocks copy them below
     if (int rc = mpd::set_field(g, c0, MPDATA_HOST)) return rc;
     std::vector<int> st[3];
     for (int a = 0; a < 3; a++) split_axis(D->n[a], D->split[a], st[a]);

@@ -358,11 +358,21 @@ template <typename T> int step_impl(Solver* h, int nsteps)
     const int P = h->order;
     for (int s = 0; s < nsteps; s++) {
         const int b0 = h->cur, b1 = (b0 + 1) % 3, b2 = (b0 + 2) % 3;
-        // pass 0: donor cell with the advective faces
+        // pass 0: donor cell with the advective faces (formed in the same march
+        // when a velocity update left them pending)
         {
             PassTimer t(h, 0);
-            op.donor(d, Cb<T>(h, b0), F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), Cb<T>(h, b1), 0,
-                     0, 0, h->stream);
+            if (h->vel_pending) {
+                const T* m = (const T*)h->metric;
+                const T* const* v = reinterpret_cast<const T* const*>(h->vel_dev);
+                op.courant_donor(d, m, m + d.nx, m + d.nx + d.ny, (T)h->vel_dt, v[0], v[1], v[2],
+                                 v[3], v[4], v[5], Cb<T>(h, b0), F<T>(h, 0, 0), F<T>(h, 0, 1),
+                                 F<T>(h, 0, 2), Cb<T>(h, b1), 0, 0, h->stream);
+                h->vel_pending = false;
+            } else {
+                op.donor(d, Cb<T>(h, b0), F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2),
+                         Cb<T>(h, b1), 0, 0, 0, h->stream);
+            }
         }
         int in = b1, out = b2;
         for (int o = 1; o < P; o++) {
@@ -443,6 +453,7 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
     const T* dev[6];
     for (int v = 0; v < 6; v++) dev[v] = (const T*)h->vel[src_of[v]];
 
+    h->vel_pending = false;  // this step forms its own faces from its own velocities
     // the fused face+donor kernel writes only the face entries the passes read
     if (!h->faces0_clean) {
         for (int a = 0; a < 3; a++) CUDA_TRY(cudaMemsetAsync(h->faces[0][a], 0, fb, h->stream));
@@ -728,26 +739,48 @@ int mpd::set_velocity(Solver* h, const void* dx, const void* dy, const void* ds,
     CUDA_TRY(cudaMemcpyAsync(met, dx, h->d.nx * h->esz, kind, h->stream));
     CUDA_TRY(cudaMemcpyAsync(met + h->d.nx * h->esz, dy, h->d.ny * h->esz, kind, h->stream));
     CUDA_TRY(cudaMemcpyAsync(met + (h->d.nx + h->d.ny) * h->esz, ds, h->d.ns * h->esz, kind, h->stream));
-    if (h->dtype == MPDATA_F32) {
-        const float* m = (const float*)h->metric;
-        ops<float>(h).courant(h->d, m, m + h->d.nx, m + h->d.nx + h->d.ny, (float)dt,
-                              (const float*)dev[0], (const float*)dev[1], (const float*)dev[2],
-                              (const float*)dev[3], (const float*)dev[4], (const float*)dev[5],
-                              F<float>(h, 0, 0), F<float>(h, 0, 1), F<float>(h, 0, 2), 0,
-                              h->d.ns, h->stream);
-    } else {
-        const double* m = (const double*)h->metric;
-        ops<double>(h).courant(h->d, m, m + h->d.nx, m + h->d.nx + h->d.ny, dt,
-                               (const double*)dev[0], (const double*)dev[1], (const double*)dev[2],
-                               (const double*)dev[3], (const double*)dev[4], (const double*)dev[5],
-                               F<double>(h, 0, 0), F<double>(h, 0, 1), F<double>(h, 0, 2), 0,
-                               h->d.ns, h->stream);
-    }
-    CUDA_TRY(cudaGetLastError());
+    for (int v = 0; v < 6; v++) h->vel_dev[v] = dev[v];
+    h->vel_dt = dt;
+    h->vel_pending = true;
     h->have_faces = true;
-    h->faces0_clean = true;  // k_courant writes every entry
+    // The next step forms the faces in its pass 0 (one march with the donor
+    // update); the Courant check and the one-kernel-per-routine path need
+    // them now.
+    if (!h->opts.check_courant && h->opts.kernel != 1) {
+        if (!h->faces0_clean) {  // the fused march writes only the used entries
+            for (int a = 0; a < 3; a++) CUDA_TRY(cudaMemsetAsync(h->faces[0][a], 0, fb, h->stream));
+            h->faces0_clean = true;
+        }
+        return 0;
+    }
+    if (int rc = materialize_faces(h)) return rc;
     if (h->opts.check_courant)
         return h->dtype == MPDATA_F32 ? check_courant<float>(h) : check_courant<double>(h);
+    return 0;
+}
+
+// The advective faces of a pending velocity update, formed now (k_courant
+// writes every entry, unused ones as 0).
+int mpd::materialize_faces(Solver* h)
+{
+    if (!h->vel_pending) return 0;
+    if (int rc = ensure_device(h)) return rc;
+    if (h->dtype == MPDATA_F32) {
+        const float* m = (const float*)h->metric;
+        const float* const* v = reinterpret_cast<const float* const*>(h->vel_dev);
+        ops<float>(h).courant(h->d, m, m + h->d.nx, m + h->d.nx + h->d.ny, (float)h->vel_dt, v[0],
+                              v[1], v[2], v[3], v[4], v[5], F<float>(h, 0, 0), F<float>(h, 0, 1),
+                              F<float>(h, 0, 2), 0, h->d.ns, h->stream);
+    } else {
+        const double* m = (const double*)h->metric;
+        const double* const* v = reinterpret_cast<const double* const*>(h->vel_dev);
+        ops<double>(h).courant(h->d, m, m + h->d.nx, m + h->d.nx + h->d.ny, h->vel_dt, v[0], v[1],
+                               v[2], v[3], v[4], v[5], F<double>(h, 0, 0), F<double>(h, 0, 1),
+                               F<double>(h, 0, 2), 0, h->d.ns, h->stream);
+    }
+    CUDA_TRY(cudaGetLastError());
+    h->vel_pending = false;
+    h->faces0_clean = true;
     return 0;
 }
 
@@ -760,6 +793,7 @@ int mpd::set_faces(Solver* h, const void* U, const void* V, const void* W, int w
         if (int rc = put_grid(h, h->faces[0][a], src[a], where)) return rc;
     h->have_faces = true;
     h->faces0_clean = false;
+    h->vel_pending = false;  // these faces supersede a pending velocity update
     if (h->opts.check_courant)
         return h->dtype == MPDATA_F32 ? check_courant<float>(h) : check_courant<double>(h);
     return 0;

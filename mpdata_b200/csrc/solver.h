@@ -44,6 +44,11 @@ struct Solver {
     // faces[0] entries no pass reads (shell rows and planes) hold 0, as
     // k_courant writes them; set_faces may leave the caller's values there.
     bool faces0_clean = true;
+    // A velocity update whose advective faces the next step's pass 0 forms
+    // (fused with the donor update); materialize_faces() forms them earlier.
+    bool vel_pending = false;
+    double vel_dt = 0;
+    const void* vel_dev[6] = {nullptr};  // staged velocity arrays (vel[])
     int zdepth = 0;  // fused kernels: planes per z chunk (set by the default heuristic / autotuner)
     // Pipelined host-array step: upload and download streams, chunk events.
     cudaStream_t s_up = nullptr, s_down = nullptr;
@@ -68,6 +73,8 @@ void destroy_solver(Solver* h);
 int set_velocity(Solver* h, const void* dx, const void* dy, const void* ds, double dt,
                  const void* const vel[6], int where);
 int set_faces(Solver* h, const void* U, const void* V, const void* W, int where);
+// Forms the advective faces of a pending velocity update now (no-op otherwise).
+int materialize_faces(Solver* h);
 int set_field(Solver* h, const void* c, int where);
 int get_field(Solver* h, void* c, int where, bool previous);
 int step(Solver* h, int nsteps);
