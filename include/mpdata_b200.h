@@ -181,9 +181,11 @@ int mpdata_set_stream(mpdata_handle h, void* stream);
 /* Velocities as in smolar() (six full-grid arrays of the handle's dtype plus
  * dx, dy, ds and dt); the advective faces are computed on the GPU, by the
  * next step's donor pass in the same kernel (at once when check_courant is
- * set or kernel = 1).  The arrays are copied in: the caller may reuse them
- * when the call returns.  `where` tells whether the pointers are host or
- * device memory. */
+ * set or kernel = 1).  The arrays are copied into the handle's own buffers
+ * in stream order: pageable host arrays may be reused when the call returns,
+ * pinned host or device arrays once the handle's stream has passed the copy
+ * (mpdata_sync).  `where` tells whether the pointers are host or device
+ * memory. */
 int mpdata_set_velocity(mpdata_handle h, const void* dx, const void* dy, const void* ds,
                         double dt, const void* u0, const void* u1, const void* v0,
                         const void* v1, const void* w0, const void* w1, int where);
