@@ -137,7 +137,10 @@ typedef struct mpdata_solver* mpdata_handle;
 #define MPDATA_F32 0
 #define MPDATA_F64 1
 
-/* Where a pointer argument lives. */
+/* Where a pointer argument lives.  A DEVICE array is read or written by a
+ * copy queued on the handle's stream: the caller orders the work that makes
+ * or reuses it with that stream (mpdata_set_stream to share one stream, or
+ * synchronise both sides). */
 #define MPDATA_HOST 0
 #define MPDATA_DEVICE 1
 /* Host memory (pinned: mpdata_host_alloc) written by a copy that is only

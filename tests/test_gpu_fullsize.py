@@ -5,7 +5,9 @@ limiter, streamfunction flow): properties that do not depend on the size.
   negative cell and stays within relative L2 1e-5 of an FP64 run of the
   plain method after 10 steps;
 * a z-chunked march gives the same bits as the whole-column one at every
-  chunk depth (chunks of 96 planes are the default here).
+  chunk depth (chunks of 96 planes are the default here);
+* a grid of more than 2^31 elements per field steps correctly (64-bit
+  offsets throughout).
 """
 import numpy as np
 import pytest
@@ -57,3 +59,48 @@ def test_fullsize_chunked_march_same_bits(m, wl, opts):
     for depth in (None, 32):
         got, _, _ = _steps(m, wl, 3, depth=depth, **opts)
         assert np.array_equal(got, ref), depth
+
+
+def test_grid_beyond_32bit_offsets(m):
+    """1024 x 1024 x 2049 cells (2.15e9 > 2^31 elements per field, ~105 GB of
+    solver state): a problem that is one-dimensional in z (U = V = 0,
+    constant W, a field varying in z only) gives every interior column the
+    same arithmetic, so each column -- the far corner's too, whose offsets
+    need 64 bits -- must equal the column of a 6 x 6 x 2049 grid bit for bit."""
+    torch = pytest.importorskip("torch")
+    ns = 2049
+    z = torch.linspace(0.0, 12.0, ns, dtype=torch.float64)
+    prof = (1.0 + torch.sin(z) * torch.exp(-0.05 * z)).to(torch.float32).cuda()
+
+    def run(nx, ny):
+        s = m.Solver(nx, ny, ns, order=2, kernel=3)  # the two-cell pass at both sizes
+        try:
+            # device arrays are read on the handle's stream: share torch's, so
+            # the copies follow the fills and precede the reuse of freed blocks
+            s.set_stream(torch.cuda.current_stream().cuda_stream)
+            shape = (ns, ny, nx)
+            zero = torch.zeros(shape, dtype=torch.float32, device="cuda")
+            W = torch.full(shape, 0.3, dtype=torch.float32, device="cuda")
+            s.set_faces(zero, zero, W)
+            del W
+            c = prof.view(ns, 1, 1).expand(shape).contiguous()
+            s.set_field(c)
+            del c, zero
+            torch.cuda.empty_cache()
+            s.step(2)
+            out = torch.empty(shape, dtype=torch.float32, device="cuda")
+            s.get_field(out)
+            s.sync()
+            cols = [out[:, 1, 1].clone(), out[:, ny // 2, nx // 2].clone(),
+                    out[:, ny - 2, nx - 2].clone()]
+            del out
+            torch.cuda.empty_cache()
+            return cols
+        finally:
+            s.close()
+
+    small = run(6, 6)
+    big = run(1024, 1024)
+    for col in big + small[1:]:
+        assert torch.equal(col, small[0])
+    assert not torch.equal(small[0], prof)  # the step moved the profile
