@@ -68,6 +68,10 @@ def test_grid_beyond_32bit_offsets(m):
     same arithmetic, so each column -- the far corner's too, whose offsets
     need 64 bits -- must equal the column of a 6 x 6 x 2049 grid bit for bit."""
     torch = pytest.importorskip("torch")
+    torch.cuda.empty_cache()
+    free, _ = torch.cuda.mem_get_info()
+    if free < 130e9:  # 103 GB of solver state + 17 GB of inputs at the peak
+        pytest.skip(f"needs 130 GB of free device memory, {free / 1e9:.0f} GB free")
     ns = 2049
     z = torch.linspace(0.0, 12.0, ns, dtype=torch.float64)
     prof = (1.0 + torch.sin(z) * torch.exp(-0.05 * z)).to(torch.float32).cuda()
