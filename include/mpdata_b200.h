@@ -146,6 +146,12 @@ typedef struct mpdata_solver* mpdata_handle;
 /* Host memory (pinned: mpdata_host_alloc) written by a copy that is only
  * queued: mpdata_get_planes() returns a ticket for mpdata_wait(). */
 #define MPDATA_HOST_ASYNC 2
+/* mpdata_set_velocity only: device arrays the handle reads in place instead
+ * of copying them, until the next mpdata_step has run on the handle's stream
+ * (the caller leaves them unchanged until then).  Taken in place when they
+ * have the handle's row pitch (nx a multiple of 32) and 16-byte alignment,
+ * copied as MPDATA_DEVICE otherwise. */
+#define MPDATA_DEVICE_BORROW 3
 
 /* Divergent-flow term of the antidiffusive velocity. */
 #define MPDATA_DIV_REFERENCE 0 /* as the reference codes it (uu.c:81-84, vv.c:85-89, ww.c:88-92) */
@@ -188,7 +194,7 @@ int mpdata_set_stream(mpdata_handle h, void* stream);
  * in stream order: pageable host arrays may be reused when the call returns,
  * pinned host or device arrays once the handle's stream has passed the copy
  * (mpdata_sync).  `where` tells whether the pointers are host or device
- * memory. */
+ * memory; MPDATA_DEVICE_BORROW lends device arrays without the copy. */
 int mpdata_set_velocity(mpdata_handle h, const void* dx, const void* dy, const void* ds,
                         double dt, const void* u0, const void* u1, const void* v0,
                         const void* v1, const void* w0, const void* w1, int where);

@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libmpdata_b200.so")
 SOLENOIDAL, DIVERGENT = 0, 1
 MSMOLAR_SERIAL, MSMOLAR_PTHREADS, MSMOLAR_OPENMP = 0, 1, 2
 F32, F64 = 0, 1
-HOST, DEVICE, HOST_ASYNC = 0, 1, 2
+HOST, DEVICE, HOST_ASYNC, DEVICE_BORROW = 0, 1, 2, 3
 DIV_REFERENCE, DIV_OFF = 0, 1
 
 ERRORS = {-1: "MPDATA_ERR_ARG", -2: "MPDATA_ERR_CUDA", -3: "MPDATA_ERR_NOMEM",
@@ -309,14 +309,20 @@ class Solver:
     def set_stream(self, stream_handle: int | None):
         _check(_lib.mpdata_set_stream(self._h, C.c_void_p(stream_handle)))
 
-    def set_velocity(self, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1):
+    def set_velocity(self, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, borrow: bool = False):
+        """``borrow``: CUDA tensors the handle reads in place until the next
+        step has run (MPDATA_DEVICE_BORROW); leave them unchanged until then."""
         ptrs = [_ptr(x, self.dtype) for x in (dx, dy, ds, u0, u1, v0, v1, w0, w1)]
         wheres = {w for _, w in ptrs}
         if len(wheres) != 1:
             raise TypeError("all velocity arguments must live in the same memory")
+        where = wheres.pop()
+        if borrow:
+            if where != DEVICE:
+                raise TypeError("only device arrays can be lent")
+            where = DEVICE_BORROW
         p = [x for x, _ in ptrs]
-        _check(_lib.mpdata_set_velocity(self._h, p[0], p[1], p[2], C.c_double(dt), *p[3:],
-                                        wheres.pop()))
+        _check(_lib.mpdata_set_velocity(self._h, p[0], p[1], p[2], C.c_double(dt), *p[3:], where))
 
     def set_faces(self, U, V, W):
         ptrs = [_ptr(x, self.dtype) for x in (U, V, W)]

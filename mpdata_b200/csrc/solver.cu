@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -220,6 +221,7 @@ int ensure_device(const Solver* h)
 // Copy a dense host/device full grid (row pitch nx) into a pitched device array.
 int put_grid(Solver* h, void* dst, const void* src, int where)
 {
+    if (where != MPDATA_HOST && where != MPDATA_DEVICE) return mpd::fail(MPDATA_ERR_ARG, "bad where %d", where);
     size_t w = (size_t)h->d.nx * h->esz;
     CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)h->d.px * h->esz, src, w, w,
                                (size_t)h->d.ny * h->d.ns,
@@ -231,6 +233,7 @@ int put_grid(Solver* h, void* dst, const void* src, int where)
 
 int get_grid(Solver* h, void* dst, const void* src, int where)
 {
+    if (where != MPDATA_HOST && where != MPDATA_DEVICE) return mpd::fail(MPDATA_ERR_ARG, "bad where %d", where);
     size_t w = (size_t)h->d.nx * h->esz;
     CUDA_TRY(cudaMemcpy2DAsync(dst, w, src, (size_t)h->d.px * h->esz, w,
                                (size_t)h->d.ny * h->d.ns,
@@ -720,12 +723,20 @@ int mpd::set_velocity(Solver* h, const void* dx, const void* dy, const void* ds,
     if (!h || !dx || !dy || !ds) return fail(MPDATA_ERR_ARG, "null argument");
     for (int v = 0; v < 6; v++)
         if (!vel[v]) return fail(MPDATA_ERR_ARG, "null velocity array");
+    if (where != MPDATA_HOST && where != MPDATA_DEVICE && where != MPDATA_DEVICE_BORROW)
+        return fail(MPDATA_ERR_ARG, "bad where %d", where);
     if (int rc = ensure_device(h)) return rc;
     const size_t fb = field_bytes(h);
+    // Lent device arrays are read in place when their layout is the handle's
+    // (dense rows of pitch nx == px, 16-byte aligned for the vector loads).
+    bool in_place = where == MPDATA_DEVICE_BORROW && h->d.px == h->d.nx;
+    for (int v = 0; v < 6 && in_place; v++) in_place = (uintptr_t)vel[v] % 16 == 0;
+    if (where == MPDATA_DEVICE_BORROW) where = MPDATA_DEVICE;
     // Stage the distinct velocity arrays (drivers pass the same array for both
     // time levels, reference tests/ring2d/test.c:89-91).
     const void* dev[6];
     for (int v = 0; v < 6; v++) {
+        if (in_place) { dev[v] = vel[v]; continue; }
         int same = -1;
         for (int w = 0; w < v; w++)
             if (vel[w] == vel[v]) same = w;

@@ -48,7 +48,7 @@ struct Solver {
     // (fused with the donor update); materialize_faces() forms them earlier.
     bool vel_pending = false;
     double vel_dt = 0;
-    const void* vel_dev[6] = {nullptr};  // staged velocity arrays (vel[])
+    const void* vel_dev[6] = {nullptr};  // staged velocity arrays (vel[]) or lent ones
     int zdepth = 0;  // fused kernels: planes per z chunk (set by the default heuristic / autotuner)
     // Pipelined host-array step: upload and download streams, chunk events.
     cudaStream_t s_up = nullptr, s_down = nullptr;

@@ -100,3 +100,53 @@ def test_set_faces_supersedes_pending_update(m):
     finally:
         s.close()
         t.close()
+
+
+@pytest.mark.parametrize("nx", [64, NX], ids=["in-place", "copied"])  # px == nx only for 64
+def test_lent_device_arrays_same_bits_as_copied(m, nx):
+    """MPDATA_DEVICE_BORROW: the step reads the caller's device arrays in place
+    (rows of pitch nx, a multiple of 32) or, for another layout, copies them;
+    either way the bits equal those of a copied update.  The lent arrays are
+    overwritten after the step has run: later steps do not read them."""
+    torch = pytest.importorskip("torch")
+    g = workloads.random_case(nx, NY, NS, seed=nx + 5)
+    f = {k: (v.astype(np.float32) if isinstance(v, np.ndarray) else v) for k, v in g.items()}
+    dev = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() if isinstance(v, np.ndarray) else v
+           for k, v in f.items()}
+    out = []
+    for borrow in (False, True):
+        s = m.Solver(nx, NY, NS, order=3, limiter=True, approx_div=True)
+        try:
+            s.set_stream(torch.cuda.current_stream().cuda_stream)
+            vel = [dev[k].clone() if isinstance(dev[k], torch.Tensor) else dev[k] for k in
+                   ("dx", "dy", "ds", "dt", "u0", "u1", "v0", "v1", "w0", "w1")]
+            s.set_velocity(*vel, borrow=borrow)
+            s.set_field(f["c0"])
+            s.step(1)
+            s.sync()
+            for t in vel:
+                if isinstance(t, torch.Tensor):
+                    t.fill_(7.0)  # the update has been consumed
+            s.step(2)
+            out.append(s.get_field())
+        finally:
+            s.close()
+    assert np.array_equal(out[0], out[1])
+
+
+def test_borrow_is_for_velocities_only(m):
+    """The other copy entry points reject MPDATA_DEVICE_BORROW (MPDATA_ERR_ARG)."""
+    import ctypes as C
+    torch = pytest.importorskip("torch")
+    s = m.Solver(NX, NY, NS, order=2)
+    try:
+        c = torch.zeros((NS, NY, NX), dtype=torch.float32, device="cuda")
+        p = C.c_void_p(c.data_ptr())
+        lib = m.library()
+        assert lib.mpdata_set_field(s._h, p, m.DEVICE_BORROW) == -1
+        assert lib.mpdata_set_faces(s._h, p, p, p, m.DEVICE_BORROW) == -1
+        assert lib.mpdata_set_field(s._h, p, m.DEVICE) == 0
+        assert lib.mpdata_get_field(s._h, p, m.DEVICE_BORROW) == -1
+        assert lib.mpdata_get_planes(s._h, 0, 1, p, m.DEVICE_BORROW) == -1
+    finally:
+        s.close()
