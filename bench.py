@@ -360,7 +360,7 @@ def run_gpu(args):
     if rank == 0 and not args.no_e2e:
         e2e = run_e2e(m, args, dict(FORMS)[chosen])
     tdep = None
-    if rank == 0 and not args.no_e2e:
+    if rank == 0 and not args.no_time_dependent:
         tdep = run_time_dependent(m, torch, dict(FORMS)[chosen])
     ens = None
     if rank == 0 and not args.no_ensemble:
@@ -748,6 +748,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-time-dependent", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")

@@ -64,6 +64,32 @@ void launch_courant(const Dims& d, const T* dx, const T* dy, const T* ds, T dt, 
                                               k0);
 }
 
+// z-chunk depth of a vector march over `planes` planes with `cols` CTAs per
+// plane and `per_sm` CTAs resident on each of the 148 SMs: the depth that
+// minimises whole waves x (planes per CTA + one plane of setup loads), so
+// that no nearly empty last wave costs a full CTA's march.
+inline int vector_march_depth(long long cols, int planes, int per_sm)
+{
+    const long long slots = 148LL * std::max(per_sm, 1);
+    int best_d = planes;
+    long long best = -1;
+    for (int dep = planes; dep >= std::min(planes, 4); dep--) {
+        const long long nch = (planes + dep - 1) / dep;
+        const long long waves = (cols * nch + slots - 1) / slots;
+        const long long t = waves * (dep + 1);
+        if (best < 0 || t < best) { best = t; best_d = dep; }
+    }
+    return best_d;
+}
+
+// CTAs of `kern` (256 threads, no dynamic shared memory) resident per SM.
+template <typename K> int resident_per_sm(K kern)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, 256, 0) != cudaSuccess || n < 1) n = 1;
+    return n;
+}
+
 template <typename T>
 void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W, T* c1,
                   int copy_shell, int zb, int ze, cudaStream_t s)
@@ -75,13 +101,11 @@ void launch_donor(const Dims& d, const T* c0, const T* U, const T* V, const T* W
     if (zb <= 0) zb = 1;
     if (ze <= 0) ze = d.ns - 1;
     if (ze <= zb) return;
-    // vector march: 32 x 8 threads of 16 bytes each; z chunks so that the grid
-    // holds about four waves of eight 256-thread CTAs on each of 148 SMs
+    // vector march: 32 x 8 threads of 16 bytes each, z chunks in whole waves
     constexpr int N = 16 / (int)sizeof(T);
+    static const int per_sm = resident_per_sm(k_donor_v<T>);
     const int gx = (int)((d.px / N + 31) / 32), gy = (d.ny - 2 + 7) / 8;
-    const long long cols = (long long)gx * gy;
-    const long long chunks = std::max(1LL, (4LL * 148 * 8 + cols - 1) / cols);
-    const int depth = std::max(4, (int)((ze - zb + chunks - 1) / chunks));
+    const int depth = vector_march_depth((long long)gx * gy, ze - zb, per_sm);
     dim3 g(gx, gy, (ze - zb + depth - 1) / depth);
     k_donor_v<T><<<g, dim3(32, 8), 0, s>>>(d, c0, U, V, W, c1, depth, zb, ze);
 }
@@ -97,13 +121,15 @@ void launch_courant_donor(const Dims& d, const T* dx, const T* dy, const T* ds, 
     if (ze <= 0) ze = d.ns - 1;
     if (ze <= zb) return;
     constexpr int N = 16 / (int)sizeof(T);
+    const bool one = u0 == u1 && v0 == v1 && w0 == w1;
+    auto kern = one ? k_courant_donor_v<T, true> : k_courant_donor_v<T, false>;
+    static const int per_sm[2] = {resident_per_sm(k_courant_donor_v<T, false>),
+                                  resident_per_sm(k_courant_donor_v<T, true>)};
     const int gx = (int)((d.px / N + 31) / 32), gy = (d.ny - 2 + 7) / 8;
-    const long long cols = (long long)gx * gy;
-    const long long chunks = std::max(1LL, (4LL * 148 * 8 + cols - 1) / cols);
-    const int depth = std::max(4, (int)((ze - zb + chunks - 1) / chunks));
+    const int depth = vector_march_depth((long long)gx * gy, ze - zb, per_sm[one]);
     dim3 g(gx, gy, (ze - zb + depth - 1) / depth);
-    k_courant_donor_v<T><<<g, dim3(32, 8), 0, s>>>(d, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, c0,
-                                                    U, V, W, c1, depth, zb, ze);
+    kern<<<g, dim3(32, 8), 0, s>>>(d, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, c0, U, V, W, c1, depth,
+                                   zb, ze);
 }
 
 template <typename T>

@@ -329,12 +329,17 @@ __global__ void __launch_bounds__(256) k_donor_v(Dims d, const T* __restrict__ c
 // k_courant writes), on interior rows of planes [zb, ze); the boundary faces
 // V(j = 0) by the j = 1 threads and W(k = 0) by a chunk starting at plane 1.
 // Face entries no pass reads (shell rows and planes) are left untouched.
+// ONE_LEVEL: u1, v1, w1 are u0, v0, w0 (drivers pass one array for both time
+// levels, reference tests/ring2d/test.c:89-91); each is loaded once and the
+// sums take the same operands in the same order, so the bits are the same.
+// The float one-level march fits 80 registers (three CTAs per SM), the
+// two-level one 128 (two).
 template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
 template <> __device__ __forceinline__ float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
 template <> __device__ __forceinline__ double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_courant_donor_v(
+template <typename T, bool ONE_LEVEL>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (ONE_LEVEL ? 3 : 2) : 1) k_courant_donor_v(
     Dims d, const T* __restrict__ dx, const T* __restrict__ dy, const T* __restrict__ ds, T dt,
     const T* __restrict__ u0, const T* __restrict__ u1, const T* __restrict__ v0,
     const T* __restrict__ v1, const T* __restrict__ w0, const T* __restrict__ w1,
@@ -361,7 +366,8 @@ __global__ void __launch_bounds__(256) k_courant_donor_v(
     long long q = cell(d, i0, j, k0);
     Vec16<T> cm = ld16(c0 + q - Z), cc = ld16(c0 + q);
     // z faces: W(k-1) from planes k-1, k; the planes k+1 are loaded per step
-    Vec16<T> wa = ld16(w0 + q - Z), wb = ld16(w1 + q - Z), wc = ld16(w0 + q), wd = ld16(w1 + q);
+    Vec16<T> wa = ld16(w0 + q - Z), wc = ld16(w0 + q);
+    Vec16<T> wb = ONE_LEVEL ? wa : ld16(w1 + q - Z), wd = ONE_LEVEL ? wc : ld16(w1 + q);
     Vec16<T> wlo;
     {
         const T rz = ratio<false>(qdt, ds[k0 - 1]);
@@ -374,8 +380,8 @@ __global__ void __launch_bounds__(256) k_courant_donor_v(
         const Vec16<T> cp = ld16(c0 + q + Z), cd = ld16(c0 + q - Y), cu = ld16(c0 + q + Y);
         const T cl = __ldg(c0 + q - 1), cr = __ldg(c0 + q + N);
         // x faces of the vector's cells and the one below its first cell
-        const Vec16<T> a0 = ld16(u0 + q), a1 = ld16(u1 + q);
-        const T a0r = __ldg(u0 + q + N), a1r = __ldg(u1 + q + N);
+        const Vec16<T> a0 = ld16(u0 + q), a1 = ONE_LEVEL ? a0 : ld16(u1 + q);
+        const T a0r = __ldg(u0 + q + N), a1r = ONE_LEVEL ? a0r : __ldg(u1 + q + N);
         Vec16<T> uf;
 #pragma unroll
         for (int e = 0; e < N; e++) {
@@ -385,10 +391,14 @@ __global__ void __launch_bounds__(256) k_courant_donor_v(
         }
         T ufl = T(0);
         if (has_l)
-            ufl = mul_rn(rxl, ((__ldg(u0 + q - 1) + a0.v[0]) + __ldg(u1 + q - 1)) + a1.v[0]);
+            {
+            const T l0 = __ldg(u0 + q - 1), l1 = ONE_LEVEL ? l0 : __ldg(u1 + q - 1);
+            ufl = mul_rn(rxl, ((l0 + a0.v[0]) + l1) + a1.v[0]);
+        }
         // y faces j+1/2 and j-1/2
-        const Vec16<T> b0 = ld16(v0 + q), b1 = ld16(v1 + q), b0u = ld16(v0 + q + Y),
-                       b1u = ld16(v1 + q + Y), b0d = ld16(v0 + q - Y), b1d = ld16(v1 + q - Y);
+        const Vec16<T> b0 = ld16(v0 + q), b0u = ld16(v0 + q + Y), b0d = ld16(v0 + q - Y);
+        const Vec16<T> b1 = ONE_LEVEL ? b0 : ld16(v1 + q), b1u = ONE_LEVEL ? b0u : ld16(v1 + q + Y),
+                       b1d = ONE_LEVEL ? b0d : ld16(v1 + q - Y);
         Vec16<T> vf, vfl;
 #pragma unroll
         for (int e = 0; e < N; e++) {
@@ -396,7 +406,7 @@ __global__ void __launch_bounds__(256) k_courant_donor_v(
             vfl.v[e] = in_x(e) ? mul_rn(ryl, ((b0d.v[e] + b0.v[e]) + b1d.v[e]) + b1.v[e]) : T(0);
         }
         // z face k+1/2
-        const Vec16<T> wp0 = ld16(w0 + q + Z), wp1 = ld16(w1 + q + Z);
+        const Vec16<T> wp0 = ld16(w0 + q + Z), wp1 = ONE_LEVEL ? wp0 : ld16(w1 + q + Z);
         const T rz = ratio<false>(qdt, ds[k]);
         Vec16<T> wf;
 #pragma unroll

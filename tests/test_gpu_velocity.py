@@ -69,6 +69,23 @@ def test_faces_in_pass0_strict_equals_oracle(m, oracle_mod, order):
     assert np.array_equal(got, c0)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64], ids=["f32", "f64"])
+@pytest.mark.parametrize("order", [1, 3])
+@pytest.mark.parametrize("opts", [dict(), dict(limiter=True, approx_div=True), dict(strict=True)],
+                         ids=["plain", "limiter-approx", "strict"])
+def test_one_level_velocities_same_bits(m, dtype, order, opts):
+    """One array per component for both time levels (as the reference's
+    drivers pass them): the fused march loads each once; faces and field are
+    the bits of the separate kernels."""
+    if dtype == np.float64 and opts.get("approx_div"):
+        pytest.skip("approx_div is a float32 form")
+    f = _case(order + 51, dtype)
+    f["u1"], f["v1"], f["w1"] = f["u0"], f["v0"], f["w0"]
+    fused = _run(m, f, order, 3, dtype, **opts)
+    eager = _run(m, f, order, 3, dtype, check_courant=True, **opts)
+    assert np.array_equal(fused[0], eager[0]) and np.array_equal(fused[1], eager[1])
+
+
 def test_later_update_supersedes_pending_one(m):
     a, b = _case(41), _case(42)
     s = m.Solver(NX, NY, NS, order=2, limiter=True)
