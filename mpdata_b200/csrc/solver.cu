@@ -398,15 +398,16 @@ template <typename T> int step_impl(Solver* h, int nsteps)
 // smolar() is bound by PCIe, not by the GPU: every call uploads the velocity
 // arrays and the field and downloads two fields.  Here the interior planes
 // are cut into chunks of D planes and three streams overlap the work:
-// the upload stream copies chunk i (velocities, field) and records an event;
-// the compute stream, once chunk i+1 has arrived, forms the faces of chunk i,
+// the upload stream copies chunk i (velocities, field, one plane past the
+// chunk) and records an event; the compute stream, once it has arrived,
 // copies its planes of the input level into the other two levels (their
-// shell), runs pass 0 on chunk i and pass o on chunk i-o (a wavefront: pass o
-// on chunk j reads pass o-1 up to chunk j+1, and a chunk of >= 4 planes holds
-// every halo plane a pass reads); when the last pass has finished a chunk
-// the download stream copies its planes of the newest and the previous level
-// to the host.  Downloads overlap the later uploads (PCIe is full duplex) and
-// the kernels overlap both.  The kernels and their plane order are those of
+// shell), forms the faces and runs pass 0 on chunk i, then every corrective
+// pass on the chunk's planes, pass o shifted down by 4 o planes (it reads
+// pass o-1 from 3 planes below its range to 1 above); the download stream
+// then copies the last pass's planes of the chunk, newest and previous
+// level, to the host.  Downloads overlap the later uploads (PCIe is full
+// duplex) and the kernels overlap both; after the last upload only one
+// chunk's passes and download remain.  The kernels and their plane order are those of
 // the unchunked step (z-chunked marches give the same bits), so the result
 // equals step() on the whole grid bit for bit.  Pinned host memory lets every
 // copy run asynchronously; pageable memory gives the same result with less
@@ -423,7 +424,13 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
     const int interior = ns - 2;
     // 16 planes: measured best on B200 for a 512 x 512 plane (8: -3 %, 32: -8 %)
     int D = chunk > 0 ? chunk : 16;
-    D = std::max(4, std::min(D, interior));
+    // Pass o runs on chunk i's planes shifted down by o * S: it reads the
+    // previous pass's output from 3 planes below its range to 1 above, so it
+    // needs nothing from chunk i+1, and the level it reads is overwritten by
+    // pass o+1 only below that (every pass of a chunk runs once the chunk has
+    // arrived).  A chunk keeps at least 4 planes for the last pass.
+    constexpr int S = 4;
+    D = std::max(std::max(4, S * (P - 1) + 4), std::min(D, interior));
     const int NC = (interior + D - 1) / D;
     auto cb = [&](int i) { return 1 + i * D; };
     auto ce = [&](int i) { return std::min(ns - 1, 1 + (i + 1) * D); };
@@ -431,8 +438,12 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
     // above it, so chunk i's compute waits for its own upload only
     auto ul = [&](int i) { return i == 0 ? 0 : ce(i - 1) + 1; };
     auto uh = [&](int i) { return i == NC - 1 ? ns : ce(i) + 1; };
-    auto dl = [&](int i) { return i == 0 ? 0 : cb(i); };  // download range: the chunk's planes
-    auto dh = [&](int i) { return i == NC - 1 ? ns : ce(i); };
+    // planes [pb, pe) of pass o on chunk i
+    auto pb = [&](int o, int i) { return i == 0 ? 1 : cb(i) - S * o; };
+    auto pe = [&](int o, int i) { return i == NC - 1 ? ns - 1 : ce(i) - S * o; };
+    // download range: the last pass's planes of the chunk (and the shell planes)
+    auto dl = [&](int i) { return i == 0 ? 0 : pb(P - 1, i); };
+    auto dh = [&](int i) { return i == NC - 1 ? ns : pe(P - 1, i); };
 
     if (!h->s_up) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_up, cudaStreamNonBlocking));
     if (!h->s_down) CUDA_TRY(cudaStreamCreateWithFlags(&h->s_down, cudaStreamNonBlocking));
@@ -508,10 +519,10 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
     if (int rc = upload(0)) return rc;
     if (NC > 1)
         if (int rc = upload(1)) return rc;
-    for (int i = 0; i < NC + P - 1; i++) {
+    for (int i = 0; i < NC; i++) {
         if (i + 2 < NC)
             if (int rc = upload(i + 2)) return rc;
-        if (i < NC) {
+        {
             CUDA_TRY(cudaStreamWaitEvent(h->stream, ev_up[i], 0));
             const size_t off = (size_t)ul(i) * plane_dev, len = (size_t)(uh(i) - ul(i)) * plane_dev;
             for (int b = 1; b < 3; b++)
@@ -523,21 +534,16 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
                              F<T>(h, 0, 2), Cb<T>(h, b1), cb(i), ce(i), h->stream);
         }
         for (int o = 1; o < P; o++) {
-            const int j = i - o;
-            if (j < 0 || j >= NC) continue;
             mpd::PassArgs<T> a = pass_args<T>(h, o, lin[o], lout[o], b0);
-            a.zbase = cb(j);
-            a.zend = ce(j);
-            if (a.zdepth >= D) a.zdepth = 0;  // the chunk in one march per column
+            a.zbase = pb(o, i);
+            a.zend = pe(o, i);
+            if (a.zdepth >= a.zend - a.zbase) a.zdepth = 0;  // one march per column
             launch_pass<T>(h, a, h->stream);
         }
-        const int j = i - (P - 1);  // chunk the last pass has finished
-        if (j >= 0 && j < NC) {
-            CUDA_TRY(cudaEventRecord(ev_done[j], h->stream));
-            CUDA_TRY(cudaStreamWaitEvent(h->s_down, ev_done[j], 0));
-            if (int rc = down(newest, h->c[cur], dl(j), dh(j))) return rc;
-            if (int rc = down(prev, h->c[prv], dl(j), dh(j))) return rc;
-        }
+        CUDA_TRY(cudaEventRecord(ev_done[i], h->stream));
+        CUDA_TRY(cudaStreamWaitEvent(h->s_down, ev_done[i], 0));
+        if (int rc = down(newest, h->c[cur], dl(i), dh(i))) return rc;
+        if (int rc = down(prev, h->c[prv], dl(i), dh(i))) return rc;
     }
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->s_down));

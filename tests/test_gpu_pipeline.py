@@ -57,7 +57,7 @@ def test_pipelined_smolar_same_bits(m, dtype, order, opt):
     m.set_default_options(m.SolverOptions(**opt))
     try:
         ref = _run(m, f, order, -1, 3, dtype)
-        for chunk in (4, 5, 7, 0):
+        for chunk in (4, 5, 7, 13, 17, 0):
             got = _run(m, f, order, chunk, 3, dtype)
             for (ga, gb), (ra, rb) in zip(got, ref):
                 assert np.array_equal(ga, ra) and np.array_equal(gb, rb), chunk
