@@ -422,8 +422,9 @@ int host_step_pipelined_impl(Solver* h, const void* dx, const void* dy, const vo
     const int ns = d.ns, P = h->order;
     const size_t esz = h->esz, fb = field_bytes(h);
     const int interior = ns - 2;
-    // 16 planes: measured best on B200 for a 512 x 512 plane (8: -3 %, 32: -8 %)
-    int D = chunk > 0 ? chunk : 16;
+    // 12 planes: measured best on B200 for a 512 x 512 plane at IORD 3
+    // (16: -0.7 %, 24: -4 %, 32: -5 %, 48: -6 %)
+    int D = chunk > 0 ? chunk : 12;
     // Pass o runs on chunk i's planes shifted down by o * S: it reads the
     // previous pass's output from 3 planes below its range to 1 above, so it
     // needs nothing from chunk i+1, and the level it reads is overwritten by
