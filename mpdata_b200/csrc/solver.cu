@@ -1025,6 +1025,8 @@ int mpdata_set_planes(mpdata_handle hh, int k0, int nk, const void* src, int whe
     if (!h || !src || nk < 0 || k0 < 0 || k0 + nk > (h ? h->d.ns : 0))
         return mpd::fail(MPDATA_ERR_ARG, "bad plane range");
     if (!h->have_field) return mpd::fail(MPDATA_ERR_STATE, "no field set");
+    if (where != MPDATA_HOST && where != MPDATA_DEVICE)
+        return mpd::fail(MPDATA_ERR_ARG, "bad where %d", where);
     if (nk == 0) return 0;
     if (int rc = ensure_device(h)) return rc;
     const size_t w = (size_t)h->d.nx * h->esz;

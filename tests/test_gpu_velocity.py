@@ -165,5 +165,6 @@ def test_borrow_is_for_velocities_only(m):
         assert lib.mpdata_set_field(s._h, p, m.DEVICE) == 0
         assert lib.mpdata_get_field(s._h, p, m.DEVICE_BORROW) == -1
         assert lib.mpdata_get_planes(s._h, 0, 1, p, m.DEVICE_BORROW) == -1
+        assert lib.mpdata_set_planes(s._h, 0, 1, p, m.DEVICE_BORROW) == -1
     finally:
         s.close()
