@@ -49,6 +49,21 @@ def faces_from_cells(u, v, w, dt=1.0):
     return U, V, W
 
 
+def cell_velocities(U, V, W):
+    """Cell velocities for the cell-velocity smolar() API whose face averages
+    (uu.c:132-134 with u0 = u1, dx = dt = 1) approximate the given faces:
+    interior cells take the mean of their two faces, ghost cells the face
+    next to them."""
+    u = np.zeros_like(U); v = np.zeros_like(V); w = np.zeros_like(W)
+    u[:, :, 1:-1] = 0.5 * (U[:, :, :-2] + U[:, :, 1:-1])
+    u[:, :, 0] = U[:, :, 0]; u[:, :, -1] = U[:, :, -2]
+    v[:, 1:-1, :] = 0.5 * (V[:, :-2, :] + V[:, 1:-1, :])
+    v[:, 0, :] = V[:, 0, :]; v[:, -1, :] = V[:, -2, :]
+    w[1:-1] = 0.5 * (W[:-2] + W[1:-1])
+    w[0] = W[0]; w[-1] = W[-2]
+    return u, v, w
+
+
 def max_courant(U, V, W) -> float:
     return float(max(np.abs(U).max(), np.abs(V).max(), np.abs(W).max()))
 

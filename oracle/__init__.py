@@ -25,7 +25,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REFERENCE_SRC = os.environ.get("MPDATA_REFERENCE_SRC", "/root/reference")
+# The reference checkout to compile from (build time only; the built files
+# travel with the tree and nothing reads the checkout at run time).
+REFERENCE_SRC = os.environ.get("MPDATA_REFERENCE_SRC")
 
 
 class OracleOpts(C.Structure):
@@ -33,16 +35,18 @@ class OracleOpts(C.Structure):
                 ("wide_beta", C.c_int)]
 
 
-def build(reference: bool = True) -> None:
-    """Compile liboracle.so, and the reference libraries when the reference
-    sources are present."""
+def build(reference: bool = True, reference_src: str | None = None) -> None:
+    """Compile liboracle.so, and the reference libraries when a reference
+    checkout is given (`reference_src`, else $MPDATA_REFERENCE_SRC) and
+    present; without one the reference build is skipped."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if reference and os.path.isdir(os.path.join(REFERENCE_SRC, "core", "src")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REFERENCE_SRC}"], check=True)
+    src = reference_src or REFERENCE_SRC
+    if reference and src and os.path.isdir(os.path.join(src, "core", "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={src}"], check=True)
         # the reference's ring drivers, also linked against the GPU library once it is built
         lib = os.path.join(os.path.dirname(HERE), "mpdata_b200", "libmpdata_b200.so")
         if os.path.exists(lib):
-            subprocess.run(["make", "-s", "-C", HERE, "drivers", f"REF={REFERENCE_SRC}"],
+            subprocess.run(["make", "-s", "-C", HERE, "drivers", f"REF={src}"],
                            check=True)
 
 
