@@ -58,24 +58,40 @@ _set_size(NX, NY, NS)
 #   corrective pass 2 reads c^(2), c^n, 3 faces; writes c^(3)                6
 B_DONOR, B_CORR_FACES, B_CORR_LAST = 5 * 4, 9 * 4, 6 * 4
 B_STEP = B_DONOR + B_CORR_FACES + B_CORR_LAST  # 80 B per cell-step
+# Ensemble (2D, IORD 2, limiter), counted as separate passes: donor reads c and
+# 2 faces, writes c (4 elements); the corrective pass reads c^(1), c^n, 2 faces
+# and writes c^(2) (5 elements).  The fused form keeps c^(1) on chip (4 elements
+# move: c^n, 2 faces in, c^(2) out).
+B_ENSEMBLE = 9 * 4
+B_ENSEMBLE_FUSED = 4 * 4
 FALLBACK_HBM_GBS = 6650.0
-# Arithmetic forms timed ("plain" = IEEE FP32 throughout); the headline value is
-# the fastest form whose result stays within the FP64 error bound.
-FORMS = [("plain", {}), ("precision_form", {"precision_form": True}),
+# Arithmetic forms timed: "plain" = IEEE FP32 throughout; "precision_form" =
+# FP32 storage and faces (hardware-reciprocal face ratios) with the limiter's
+# sums and ratios in FP64; "approx_div" = FP32 with hardware-reciprocal ratios
+# everywhere.  The headline value is the fastest form within the FP64 error
+# bound (see the selection below).
+FORMS = [("plain", {}), ("precision_form", {"precision_form": True, "approx_div": True}),
          ("approx_div", {"approx_div": True})]
 FP64_REL_L2_BOUND = 1e-5
+# Options of the throughput workload beside the form: the y faces of the x = 1
+# column are computed (vv_fix).  The reference leaves them unwritten
+# (vv.c:81-82): its first corrective pass reads an uninitialised buffer there
+# and, with IORD 3, its second one applies the advective velocity as an
+# antidiffusive one in that column.  The accuracy check reports that rule too.
+WORKLOAD_OPTS = {"vv_fix": True}
 ACC_STEPS = 100  # horizon of the FP64 accuracy check: the configuration's length
 # The corrective-pass kernel each form runs (the solver's default kernel choice).
 KERNEL_OF_FORM = {
     "plain": "k_pass_tma<float, limiter> (fused corrective pass, one cell per thread)",
-    "precision_form": "k_pass_tma<float, limiter, double ratios> (fused, one cell per thread)",
+    "precision_form": "k_pass_pair<limiter, approx, FP64 limiter ratios> (fused corrective pass, "
+                      "two cells per thread)",
     "approx_div": "k_pass_pair<limiter, approx> (fused corrective pass, two cells per thread)",
 }
 
 
 def config_text():
     return (f"roofline: {NX}x{NY}x{NS} FP32, IORD {ORDER} + nonoscillatory limiter, "
-            "streamfunction flow")
+            "streamfunction flow, y faces of the x = 1 column computed (vv_fix)")
 
 
 def hbm_peak():
@@ -272,7 +288,7 @@ def run_gpu(args):
 
     def timed_form(opts):
         """W untimed steps, then EXACTLY K timed steps of one arithmetic form."""
-        s = m.Solver(NX, NY, NS, order=ORDER, limiter=True, **opts)
+        s = m.Solver(NX, NY, NS, order=ORDER, limiter=True, **WORKLOAD_OPTS, **opts)
         s.set_stream(stream.cuda_stream)
         s.set_faces(wl["U"], wl["V"], wl["W"])
         s.set_field(wl["c0"])
@@ -310,8 +326,8 @@ def run_gpu(args):
 
     results = {name: timed_form(o) for name, o in FORMS}
 
-    def fp64_run(nsteps, c0=None):
-        s64 = m.Solver(NX, NY, NS, order=ORDER, dtype=np.float64, limiter=True)
+    def fp64_run(nsteps, c0=None, **wopts):
+        s64 = m.Solver(NX, NY, NS, order=ORDER, dtype=np.float64, limiter=True, **wopts)
         s64.set_stream(stream.cuda_stream)
         s64.set_faces(*(wl[k].astype(np.float64) for k in ("U", "V", "W")))
         s64.set_field(wl["c0"].astype(np.float64) if c0 is None else c0)
@@ -330,19 +346,29 @@ def run_gpu(args):
     # scheme's own sensitivity: the same FP64 run started from c0 perturbed
     # by half an FP32 ulp (relative) per cell -- the error any FP32-storage
     # form incurs by rounding the field once.
-    ref64 = fp64_run(ACC_STEPS)
-    nref = float(np.linalg.norm(ref64))
-    acc = {}
-    for name, o in FORMS:
-        s = m.Solver(NX, NY, NS, order=ORDER, limiter=True, **o)
+    def form_run(o, nsteps, **wopts):
+        s = m.Solver(NX, NY, NS, order=ORDER, limiter=True, **wopts, **o)
         s.set_stream(stream.cuda_stream)
         s.set_faces(wl["U"], wl["V"], wl["W"])
         s.set_field(wl["c0"])
-        s.step(ACC_STEPS)
-        acc[name] = rel(s.get_field(), ref64, nref)
+        s.step(nsteps)
+        out = s.get_field()
         s.close()
-    floor = rel(fp64_run(ACC_STEPS, half_ulp_perturbed(wl["c0"])), ref64, nref)
-    ref64 = fp64_run(args.warmup + args.steps)
+        return out
+
+    ref64 = fp64_run(ACC_STEPS, **WORKLOAD_OPTS)
+    nref = float(np.linalg.norm(ref64))
+    acc = {name: rel(form_run(o, ACC_STEPS, **WORKLOAD_OPTS), ref64, nref) for name, o in FORMS}
+    floor = rel(fp64_run(ACC_STEPS, half_ulp_perturbed(wl["c0"]), **WORKLOAD_OPTS), ref64, nref)
+    # the reference's column rule (y faces of x = 1 unwritten), same horizon
+    ref64 = fp64_run(ACC_STEPS)
+    nref = float(np.linalg.norm(ref64))
+    ref_rule = {}
+    for name, o in FORMS:
+        b, _ = error_breakdown(form_run(o, ACC_STEPS), ref64, nref)
+        ref_rule[name] = {k: b[k] for k in ("rel_l2", "max_abs", "share_column_x1",
+                                            "rel_l2_without_x_le_2")}
+    ref64 = fp64_run(args.warmup + args.steps, **WORKLOAD_OPTS)
     nref = float(np.linalg.norm(ref64))
     forms = {}
     for name, r in results.items():
@@ -426,6 +452,11 @@ def run_gpu(args):
         f"{ACC_STEPS} steps from c0 (rel_l2_vs_fp64) and no negative cell; when no FP32 form "
         "meets it, the fastest form no less accurate than the plain FP32 method")
     line["fp64_bound_met"] = bound_met
+    line["reference_column_rule_accuracy"] = {
+        "steps": ACC_STEPS, "forms": ref_rule,
+        "how": "the same forms and FP64 run with the reference's rule for the y faces of the "
+               "x = 1 column (unwritten by vv.c:81-82: 0 on odd passes, the advective face on "
+               "even ones); share_column_x1 = share of the squared error in that column"}
     line["fp64_sensitivity_floor"] = {
         "rel_l2": floor[0], "max_abs": floor[1], "steps": ACC_STEPS,
         "how": "FP64 run from c0 perturbed by a seeded relative +-2^-24 (half an FP32 ulp) "
@@ -506,6 +537,8 @@ def run_ensemble(m, torch, steps: int, base_steps: int):
         s.close()
     ens_rate = cells * steps / (t_ens * 1e-3) / 1e9
     seq_rate = cells * base_steps / (t_seq * 1e-3) / 1e9
+    peak, peak_kind = hbm_peak()
+    ens_gbs = ens_rate * B_ENSEMBLE  # Gcell-steps/s x bytes per cell-step = GB/s
     return {"value": ens_rate, "unit": UNIT, "instances": len(cfg), "steps": steps,
             "interior_cells_per_step": cells, "ms_per_step": t_ens / steps,
             "tile": list(m.Ensemble.TILES[tile]), "autotune_ms_per_step": tune_ms,
@@ -513,6 +546,15 @@ def run_ensemble(m, torch, steps: int, base_steps: int):
                            "ms_per_step": t_seq / base_steps,
                            "how": "256 per-instance solvers (nx x ny x 3), stepped one after another"},
             "speedup_vs_sequential": ens_rate / seq_rate,
+            "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ENSEMBLE,
+                         "achieved": ens_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": ens_gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "fused_bytes_per_cell_step": B_ENSEMBLE_FUSED,
+                         "frac_of_fused_bytes": ens_rate * B_ENSEMBLE_FUSED / peak,
+                         "note": "whole step; bytes_per_cell_step counts the donor and "
+                                 "corrective passes separately, fused_bytes_per_cell_step the "
+                                 "one fused launch (c^(1) stays on chip); the arena partly "
+                                 "fits in the 126 MB L2"},
             "min_interior_value": min(mins)}
 
 
@@ -575,6 +617,19 @@ def run_adjoint(m, torch, nsteps: int = 200, every: int = 20, ndir: int = 32):
         if dt is np.float32:
             out["t_fwd_recording_ms_per_step"] = t_f / nsteps
             out["t_adj_ms_per_step"] = t_b / nsteps
+            # the reverse scatter-adds are atomic: a second sweep of the same
+            # window sums in another order
+            g2 = a.backward(lam).astype(np.float64)
+            out["fp32_adjoint_run_to_run_rel_l2"] = float(
+                np.linalg.norm(g2 - grads["float32"]) / np.linalg.norm(grads["float32"]))
+        else:
+            # the FP64 adjoint's own sensitivity: the same window from c0
+            # perturbed by half an FP32 ulp per cell (one rounding to FP32)
+            cp = half_ulp_perturbed(c0)
+            cNp = a.forward(np.ascontiguousarray(cp), nsteps)
+            gp = a.backward(np.ascontiguousarray(lam_of(cNp))).astype(np.float64)
+            out["fp64_adjoint_half_ulp_sensitivity_rel_l2"] = float(
+                np.linalg.norm(gp - grads["float64"]) / np.linalg.norm(grads["float64"]))
         a.close()
     # production forward step (fused kernels) on the same problem
     s = m.Solver(n, n, ns, order=2, limiter=True)
@@ -629,7 +684,7 @@ def run_time_dependent(m, torch, form_opts, steps: int = 20):
     vel = [[dev(u), dev(v), dev(w)], [dev(0.9 * u), dev(0.9 * v), dev(0.9 * w)]]
     dxyz = [dev(np.ones(n, np.float32)) for n in (NX, NY, NS)]
     stream = torch.cuda.current_stream()
-    s = m.Solver(NX, NY, NS, order=ORDER, limiter=True, **form_opts)
+    s = m.Solver(NX, NY, NS, order=ORDER, limiter=True, **WORKLOAD_OPTS, **form_opts)
     try:
         s.set_stream(stream.cuda_stream)
         s.set_field(wl["c0"])
@@ -683,7 +738,7 @@ def run_e2e(m, args, form_opts):
     bufs = [pinned(x) for x in (u, v, w, wl["c0"], np.zeros_like(wl["c0"]))]
     hu, hv, hw, c0, c1 = (b for b, _ in bufs)
     dx = np.ones(NX, np.float32); dy = np.ones(NY, np.float32); ds = np.ones(NS, np.float32)
-    m.set_default_options(m.SolverOptions(limiter=True, **form_opts))
+    m.set_default_options(m.SolverOptions(limiter=True, **WORKLOAD_OPTS, **form_opts))
     steps = max(1, min(args.steps, args.e2e_steps))
     try:
         for it in range(2 + steps):
@@ -742,10 +797,15 @@ def error_breakdown(a, ref, nref, ref_interior=None):
     """Relative L2 / max-abs of a against ref, and where the error sits:
     the share of the squared error carried by the largest 0.01 %, 0.1 % and
     1 % of the per-cell errors."""
-    e = np.abs(a.astype(np.float64) - ref).ravel()
+    e3 = np.abs(a.astype(np.float64) - ref)
+    e = e3.ravel()
     tot = float(np.dot(e, e))
+    x1 = float(np.sum(e3[:, :, 1] ** 2))
+    inner = e3[:, :, 3:]
     out = {"rel_l2": float(np.sqrt(tot)) / nref, "max_abs": float(e.max()),
-           "negative_cells": int(np.count_nonzero(a < 0))}
+           "negative_cells": int(np.count_nonzero(a < 0)),
+           "share_column_x1": x1 / tot if tot > 0 else 0.0,
+           "rel_l2_without_x_le_2": float(np.sqrt(np.sum(inner ** 2))) / nref}
     for frac in (1e-4, 1e-3, 1e-2):
         k = max(1, int(e.size * frac))
         top = np.partition(e, e.size - k)[e.size - k:]
@@ -781,8 +841,9 @@ def run_accuracy(args):
     wl = _workload()
     stream = torch.cuda.current_stream()
 
-    def run(dtype, c0, limiter=True, round_each=False, **opts):
-        s = m.Solver(NX, NY, NS, order=ORDER, dtype=dtype, limiter=limiter, **opts)
+    def run(dtype, c0, limiter=True, round_each=False, vv_fix=False, **opts):
+        s = m.Solver(NX, NY, NS, order=ORDER, dtype=dtype, limiter=limiter, vv_fix=vv_fix,
+                     **opts)
         s.set_stream(stream.cuda_stream)
         s.set_faces(*(np.ascontiguousarray(wl[k], dtype) for k in ("U", "V", "W")))
         s.set_field(np.ascontiguousarray(c0, dtype))
@@ -801,32 +862,38 @@ def run_accuracy(args):
             s.close()
 
     c0 = wl["c0"].astype(np.float64)
-    refs = {True: {mk: f for mk, f in run(np.float64, c0)},
-            False: {mk: f for mk, f in run(np.float64, c0, limiter=False)}}
-    norms = {lim: {mk: float(np.linalg.norm(f)) for mk, f in r.items()} for lim, r in refs.items()}
+    # references by (limiter, column rule): vv_fix computes the y faces of the
+    # x = 1 column (vv.c:81-82 leaves them unwritten)
+    refs = {(True, False): {mk: f for mk, f in run(np.float64, c0)},
+            (False, False): {mk: f for mk, f in run(np.float64, c0, limiter=False)},
+            (True, True): {mk: f for mk, f in run(np.float64, c0, vv_fix=True)}}
+    norms = {key: {mk: float(np.linalg.norm(f)) for mk, f in r.items()} for key, r in refs.items()}
     pert = half_ulp_perturbed(wl["c0"])
     cases = [("fp64_half_ulp_perturbed_c0", dict(dtype=np.float64, c0=pert)),
              ("fp64_rounded_to_fp32_each_step", dict(dtype=np.float64, c0=c0, round_each=True)),
              ("fp64_no_limiter_half_ulp_perturbed_c0",
-              dict(dtype=np.float64, c0=pert, limiter=False))]
+              dict(dtype=np.float64, c0=pert, limiter=False)),
+             ("fp64_vv_fix_half_ulp_perturbed_c0", dict(dtype=np.float64, c0=pert, vv_fix=True))]
     cases += [(f"fp32_{name}", dict(dtype=np.float32, c0=wl["c0"], **o)) for name, o in FORMS]
+    cases += [(f"fp32_vv_fix_{name}", dict(dtype=np.float32, c0=wl["c0"], vv_fix=True, **o))
+              for name, o in FORMS]
     rng = np.random.default_rng(3)
     sample = rng.integers(0, c0.size, 1_000_000)
     out = {"workload": config_text(), "steps": list(ACC_MARKS),
            "reference": "FP64 run of the plain method (IEEE division), same limiter setting",
            "local_extremum_fraction_all_cells": float(
-               local_extremum(refs[True][ACC_MARKS[-1]], sample).mean()),
+               local_extremum(refs[(True, False)][ACC_MARKS[-1]], sample).mean()),
            "cases": {}}
     for name, kw in cases:
-        lim = kw.get("limiter", True)
+        key = (kw.get("limiter", True), kw.get("vv_fix", False))
         res = {}
         for mk, f in run(**kw):
-            b, e = error_breakdown(f, refs[lim][mk], norms[lim][mk])
+            b, e = error_breakdown(f, refs[key][mk], norms[key][mk])
             if mk == ACC_MARKS[-1]:
                 k = max(1, int(e.size * 1e-4))
                 hot = np.argpartition(e, e.size - k)[e.size - k:]
                 b["top_0.0001_local_extremum_fraction"] = float(
-                    local_extremum(refs[lim][mk], hot).mean())
+                    local_extremum(refs[key][mk], hot).mean())
             res[mk] = b
         out["cases"][name] = res
         print(json.dumps({name: res}), file=sys.stderr, flush=True)
@@ -872,6 +939,8 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="run only the batched-ensemble configuration")
     ap.add_argument("--accuracy", action="store_true",
                     help="print the FP64 error breakdown of the FP32 forms (no timing)")
     ap.add_argument("--size", default=None,
@@ -883,6 +952,12 @@ def main():
         args.warmup = 3
     if args.accuracy:
         print(json.dumps(run_accuracy(args)), flush=True)
+        return
+    if args.ensemble_only:  # the batched-ensemble configuration alone (profiling captures)
+        import torch
+        import mpdata_b200 as m
+        torch.cuda.set_device(0)
+        print(json.dumps(run_ensemble(m, torch, args.ensemble_steps, 2)), flush=True)
         return
     line = run_reference(args) if args.impl == "reference" else run_gpu(args)
     if line is not None:

@@ -169,7 +169,7 @@ typedef struct mpdata_options {
                            below for the options (default); 1: one kernel per
                            reference function (slower; cross-check path);
                            2: fused, one cell per thread; 3: fused, two cells per
-                           thread (F32 without strict or precision_form) */
+                           thread (F32 without strict) */
     int check_courant;  /* 1: reject advective faces with |Courant| > 1 */
     int approx_div;     /* 1 (F32, fused kernels, not strict): the ratios of the
                            antidiffusive velocity and of the limiter use the

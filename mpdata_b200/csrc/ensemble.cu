@@ -110,12 +110,16 @@ void launch_step_passes(mpdata_ensemble* e, int& cur, int& prev)
     p.in = b0; p.out = b1; p.cn = b0; p.rs = 0; p.ws = 0; p.pass = 0;
     p.use_div = e->opts.div_mode != MPDATA_DIV_OFF;
     p.vv_fix = e->opts.vv_fix;
-    if (STRICT)
-        mpd::strict::launch_ens_donor<float>(e->tile, e->arena, e->insts, e->items[e->tile][0],
-                                             e->nitems[e->tile][0], e->grid_donor, p, e->stream);
-    else
-        mpd::fast::launch_ens_donor<float>(e->tile, e->arena, e->insts, e->items[e->tile][0],
-                                           e->nitems[e->tile][0], e->grid_donor, p, e->stream);
+    p.fuse_donor = 0;
+    // With corrective passes, pass 1 forms c^(1) itself (level b1 is then not written)
+    if (P == 1) {
+        if (STRICT)
+            mpd::strict::launch_ens_donor<float>(e->tile, e->arena, e->insts, e->items[e->tile][0],
+                                                 e->nitems[e->tile][0], e->grid_donor, p, e->stream);
+        else
+            mpd::fast::launch_ens_donor<float>(e->tile, e->arena, e->insts, e->items[e->tile][0],
+                                               e->nitems[e->tile][0], e->grid_donor, p, e->stream);
+    }
     int in = b1, out = b2;
     for (int o = 1; o < P; o++) {
         p.in = in; p.out = out; p.cn = b0;
@@ -123,6 +127,7 @@ void launch_step_passes(mpdata_ensemble* e, int& cur, int& prev)
         p.ws = 1 + ((o - 1) & 1);
         p.pass = o;
         p.write_faces = o < P - 1;
+        p.fuse_donor = o == 1;
         if (STRICT)
             mpd::strict::launch_ens_pass<float>(e->tile, e->arena, e->insts, e->items[e->tile][1],
                                                 e->nitems[e->tile][1], e->grid_pass, p,

@@ -10,8 +10,9 @@
 // Work list: (instance, tile) items over the instances' interior cells.  A
 // persistent grid of CTAs walks the list (item = blockIdx.x + n * gridDim.x).
 // The corrective pass stages each item's tile with a halo of 3 into shared
-// memory by cp.async, double-buffered (the next item's copies run while the
-// current item computes), forms the faces of every cell of the tile (and,
+// memory by 16-byte cp.async chunks (rows rounded down to a 16-byte
+// boundary), double-buffered (the next item's copies run while the current
+// item computes); the first corrective pass forms c^(1) itself (FUSE0), forms the faces of every cell of the tile (and,
 // with the limiter, their ratios) and updates the cells it owns: all but the
 // first column and row (the first two and the last with the limiter), so
 // every face an owned cell reads is the high face of a tile cell.  Tile shape
@@ -103,20 +104,15 @@ __device__ __forceinline__ T face_v2(const Nb2<T>& n, int i, int j, int ny, int 
     return t - T(0.5) * (n.v * ratio<AP>(ub * n1, d1));
 }
 
-// Asynchronous 4- or 8-byte copy global -> shared (cp.async, bypassing
-// registers); n_src = 0 copies nothing and fills the element with zeros.
-template <typename T>
-__device__ __forceinline__ void cp_async_el(T* dst, const T* src, bool valid)
+// Asynchronous 16-byte copy global -> shared (cp.async.cg, bypassing
+// registers and L1); valid = false copies nothing and fills the 16 bytes with
+// zeros.  Both addresses must be 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid)
 {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    if constexpr (sizeof(T) == 4)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(s), "l"(src),
-                     "r"(valid ? 4 : 0)
-                     : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(src),
-                     "r"(valid ? 8 : 0)
-                     : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait()
@@ -149,13 +145,22 @@ __global__ void __launch_bounds__(TX * TY)
 }
 
 // Corrective pass (antidiffusive faces + optional limiter + donor update), 2D.
-template <typename T, bool LIM, typename A, bool AP, int TX, int TY>
+// FUSE0 (first corrective pass only): the tile's c^(1) is formed here from the
+// staged c^n and advective faces by the donor update (k_ens_donor's
+// arithmetic, same order), so pass 0 needs no launch of its own and c^(1)
+// never goes through global memory.
+template <typename T, bool LIM, typename A, bool AP, int TX, int TY, bool FUSE0>
 __global__ void __launch_bounds__(TX * TY)
     k_ens_pass(T* __restrict__ arena, const EnsInst* __restrict__ insts,
                const EnsItem* __restrict__ items, int nitems, EnsPass p)
 {
     using namespace ens;
-    constexpr int SX = TX + 2 * H, SY = TY + 2 * H, PL = SX * SY;
+    // Staged rows start on a 16-byte boundary (x rounded down by rx < V
+    // elements) and hold whole 16-byte chunks: TX + 2H cells plus the
+    // alignment slack, rounded up to V elements.
+    constexpr int V = 16 / (int)sizeof(T);
+    constexpr int SX = (TX + 2 * H + V - 1 + V - 1) / V * V, SY = TY + 2 * H, PL = SX * SY;
+    constexpr int CH = SX / V;  // 16-byte chunks per staged row
     constexpr int NT = TX * TY;
     // Owned cells: local x in [LO, TX-1-HI] (likewise y).  The halo cells are
     // the ones whose high faces (and, with the limiter, ratios) the owned
@@ -164,30 +169,39 @@ __global__ void __launch_bounds__(TX * TY)
     constexpr int WX = TX + 2, WPL = WX * (TY + 2);  // work planes: local [-1, TX] x [-1, TY]
     // Stage buffers, double-buffered: the next item's tile is copied in
     // (cp.async) while the current one is computed.
-    __shared__ T bC[2][PL], bU[2][PL], bV[2][PL], bN[2][LIM ? PL : 1];
+    // (fused: c^n is staged in bN, c^(1) formed into bC[0])
+    constexpr bool STAGE_N = LIM || FUSE0;
+    __shared__ __align__(16) T bC[FUSE0 ? 1 : 2][PL];
+    __shared__ __align__(16) T bU[2][PL];
+    __shared__ __align__(16) T bV[2][PL];
+    __shared__ __align__(16) T bN[2][STAGE_N ? PL : V];
     __shared__ T sRU[WPL], sRV[WPL], sBU[LIM ? WPL : 1], sBD[LIM ? WPL : 1];
     const int x = threadIdx.x, y = threadIdx.y, tid = y * TX + x;
-    const int o = (y + H) * SX + (x + H);
     const int w = (y + 1) * WX + (x + 1);
 
-    // Queue the copies of item `it`'s tile (cells outside the instance read 0).
+    // Queue the copies of item `it`'s tile.  Rows of every instance array start
+    // 128-byte aligned and are padded to px (a multiple of 32) with zeros that
+    // no kernel writes, so a chunk is either inside a row (cells past nx read
+    // 0) or wholly outside the instance (zero-filled): every cell outside the
+    // instance reads 0.
     auto stage = [&](int it, int b) {
         const EnsItem item = items[it];
         const EnsInst& in = insts[item.inst];  // fields read in place (no local copy)
-        const int i0 = item.i0 - LO, j0 = item.j0 - LO;
+        const int gx0 = (item.i0 - LO - H) & ~(V - 1), gy0 = item.j0 - LO - H;
         const T* gc = arena + in.c[p.in];
         const T* gn = arena + in.c[p.cn];
         const T* gu = arena + in.f[p.rs][0];
         const T* gv = arena + in.f[p.rs][1];
-        for (int e = tid; e < PL; e += NT) {
-            const int sy = e / SX, sx = e - sy * SX;
-            const int gi = i0 - H + sx, gj = j0 - H + sy;
-            const bool inside = gi >= 0 && gi < in.nx && gj >= 0 && gj < in.ny;
+        for (int e = tid; e < CH * SY; e += NT) {
+            const int sy = e / CH, cx = e - sy * CH;
+            const int gi = gx0 + cx * V, gj = gy0 + sy;
+            const bool inside = gi >= 0 && gi < in.px && gj >= 0 && gj < in.ny;
             const long long q = inside ? (long long)gj * in.px + gi : 0;
-            cp_async_el(&bC[b][e], gc + q, inside);
-            cp_async_el(&bU[b][e], gu + q, inside);
-            cp_async_el(&bV[b][e], gv + q, inside);
-            if (LIM) cp_async_el(&bN[b][e], gn + q, inside);
+            const int d = sy * SX + cx * V;
+            if (!FUSE0) cp_async16(&bC[b][d], gc + q, inside);
+            cp_async16(&bU[b][d], gu + q, inside);
+            cp_async16(&bV[b][d], gv + q, inside);
+            if (STAGE_N) cp_async16(&bN[b][d], gn + q, inside);
         }
         cp_async_commit();
     };
@@ -202,7 +216,7 @@ __global__ void __launch_bounds__(TX * TY)
             cp_async_wait<0>();
         }
         __syncthreads();  // this item's tile has landed for every thread
-        const T* sC = bC[b];
+        const T* sC = bC[FUSE0 ? 0 : b];
         const T* sU = bU[b];
         const T* sV = bV[b];
         const T* sN = bN[b];
@@ -211,6 +225,27 @@ __global__ void __launch_bounds__(TX * TY)
         const int nx = in.nx, ny = in.ny, px = in.px;
         const int i0 = item.i0 - LO, j0 = item.j0 - LO;  // global cell of local (0, 0)
         const T* vadv = arena + in.f[0][1];
+        const int rx = (i0 - H) - ((i0 - H) & ~(V - 1));  // alignment slack of this tile
+        const int o = (y + H) * SX + (x + H) + rx;
+        if constexpr (FUSE0) {
+            // c^(1) over local [-1, TX] x [-1, TY] (every cell the pass reads):
+            // the donor update of interior cells, the fixed shell copied, 0 outside
+            T* c1 = bC[0];
+            for (int e = tid; e < (TX + 2) * (TY + 2); e += NT) {
+                const int ly = e / (TX + 2) - 1, lx = e - (ly + 1) * (TX + 2) - 1;
+                const int q = (ly + H) * SX + (lx + H) + rx;
+                const int gi = i0 + lx, gj = j0 + ly;
+                T v = sN[q];
+                if (gi >= 1 && gi <= nx - 2 && gj >= 1 && gj <= ny - 2) {
+                    const T cc = sN[q];
+                    const T fx = upwind(cc, sN[q + 1], sU[q]) - upwind(sN[q - 1], cc, sU[q - 1]);
+                    const T fy = upwind(cc, sN[q + SX], sV[q]) - upwind(sN[q - SX], cc, sV[q - SX]);
+                    v = cc - T(0.5) * (fx + fy);
+                }
+                c1[q] = v;
+            }
+            __syncthreads();
+        }
 
         const int i = i0 + x, j = j0 + y;
         const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
@@ -279,7 +314,12 @@ template <typename T, bool LIM, typename A, bool AP, int TX, int TY>
 void ens_launch_pass(T* arena, const EnsInst* insts, const EnsItem* items, int nitems, int grid,
                      const EnsPass& p, cudaStream_t s)
 {
-    k_ens_pass<T, LIM, A, AP, TX, TY><<<grid, dim3(TX, TY), 0, s>>>(arena, insts, items, nitems, p);
+    if (p.fuse_donor)
+        k_ens_pass<T, LIM, A, AP, TX, TY, true><<<grid, dim3(TX, TY), 0, s>>>(arena, insts, items,
+                                                                              nitems, p);
+    else
+        k_ens_pass<T, LIM, A, AP, TX, TY, false><<<grid, dim3(TX, TY), 0, s>>>(arena, insts, items,
+                                                                               nitems, p);
 }
 
 template <typename T, int TX, int TY>

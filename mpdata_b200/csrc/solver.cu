@@ -174,10 +174,12 @@ int default_zdepth(const mpd::Solver* h)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     const bool lim = h->opts.limiter != 0;
-    int sx, sy, per_sm;
+    int sx, sy, per_sm, cl = 1;
     if (h->pair) {
         sx = lim ? 28 : 30;
-        sy = lim ? mpd::kPairCY - 3 : mpd::kPairCY - 1;
+        // with the limiter, clusters of kPairCL CTAs advance pair_rows_per_cluster() rows
+        sy = lim ? mpd::pair_rows_per_cluster() : mpd::kPairCY - 1;
+        cl = lim ? mpd::kPairCL : 1;
         per_sm = mpd::kPairCY >= 32 ? 1 : 2;
     } else {
         sx = lim ? 30 : 32;
@@ -185,7 +187,7 @@ int default_zdepth(const mpd::Solver* h)
         per_sm = 2;
     }
     const long long bx = (h->d.nx - 2 + sx - 1) / sx;
-    const long long by = (h->d.ny - 2 + sy - 1) / sy;
+    const long long by = cl * ((h->d.ny - 2 + sy - 1) / sy);
     const long long want = 6LL * per_sm * sms;
     const int interior = h->d.ns - 2;
     long long chunks = (want + bx * by - 1) / (bx * by);
@@ -682,8 +684,8 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     if (o.precision_form && dtype != MPDATA_F32)
         return fail(MPDATA_ERR_ARG, "precision_form applies to float storage only");
     if (o.kernel < 0 || o.kernel > 3) return fail(MPDATA_ERR_ARG, "bad kernel option %d", o.kernel);
-    if (o.kernel == 3 && (dtype != MPDATA_F32 || o.strict || o.precision_form))
-        return fail(MPDATA_ERR_ARG, "the two-cell pass needs float storage without strict or precision_form");
+    if (o.kernel == 3 && (dtype != MPDATA_F32 || o.strict))
+        return fail(MPDATA_ERR_ARG, "the two-cell pass needs float storage without strict mode");
     if (o.approx_div && (dtype != MPDATA_F32 || o.strict || o.kernel == 1))
         return fail(MPDATA_ERR_ARG, "approx_div needs float storage, fused kernels and no strict mode");
     std::unique_ptr<Solver> h(new Solver());
@@ -699,11 +701,12 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     CUDA_TRY(cudaGetDevice(&h->device));
     CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
-    // The two-cell pass: FP32, fast arithmetic, FP32 limiter ratios, fused kernels by
-    // default.  With the limiter and IEEE division the one-cell pass is faster on B200
-    // (the division slow paths spill the two-cell kernel's registers), so it keeps it.
-    h->pair = o.kernel == 3 || (dtype == MPDATA_F32 && !o.strict && !o.precision_form &&
-                                o.kernel == 0 && (o.approx_div || !o.limiter));
+    // The two-cell pass: FP32, fast arithmetic, fused kernels by default (with
+    // precision_form its limiter sums and ratios run in FP64).  With the limiter and
+    // IEEE division the one-cell pass is faster on B200 (the division slow paths
+    // spill the two-cell kernel's registers), so it keeps that form.
+    h->pair = o.kernel == 3 || (dtype == MPDATA_F32 && !o.strict && o.kernel == 0 &&
+                                (o.approx_div || !o.limiter));
     h->zdepth = default_zdepth(h.get());
     if (int rc = alloc_solver(h.get())) {
         free_solver(h.get());

@@ -137,3 +137,76 @@ def test_torch_harness_receptor_inversion():
         fd = (loss64(1.3, e * v) - loss64(1.3, -e * v)) / (2 * e)
         ad = float(np.sum(g_c0 * v))
         assert abs(fd - ad) <= 1e-4 * max(abs(fd), 1e-6) + 1e-7
+
+
+def _c5_problem():
+    """The adjoint configuration: 128x128x64, ring3d-type flow (rotation about
+    z, max Courant 0.4, uniform w 0.1), Gaussian blob on a smoothly varying
+    background, 64 seeded receptors against a target from another blob."""
+    n, ns = 128, 64
+    r = workloads.ring3d(n=n, ns=ns, courant=0.4, wcourant=0.1, sigma=6.0, offset=30.0,
+                         background=1e-6)
+    tr = workloads.ring3d(n=n, ns=ns, courant=0.4, wcourant=0.1, sigma=8.0, offset=-25.0,
+                          background=1e-6)["c0"]
+    faces = workloads.faces_from_cells(r["u"], r["v"], r["w"])
+    k, j, i = np.mgrid[0:ns, 0:n, 0:n].astype(np.float64)
+    c0 = r["c0"] + 1e-4 * (1.5 + np.sin(0.3 * i) * np.cos(0.25 * j + 0.2 * k))
+    rng = np.random.default_rng(workloads.SEED + 5)
+    rec = rng.integers(0, c0.size, 64)
+    return faces, c0, rec, tr.reshape(-1)[rec], rng
+
+
+def test_c5_window_adjoint():
+    """The adjoint configuration at its size and length (200 steps,
+    checkpoint every 20, IORD 2 + limiter with frozen branches):
+
+    * FP64 adjoint against FP64 central differences along 8 random
+      directions: median relative error <= 1e-5;
+    * FP32 adjoint against the FP64 adjoint: relative L2 <= 0.1 and no more
+      than 3x the FP64 adjoint's own change when c0 moves by half an FP32 ulp
+      per cell (the limiter's selections move with the rounding);
+    * two FP32 reverse sweeps of the same window agree to relative L2 1e-5
+      (the scatter-adds are atomic, so their summation order varies)."""
+    import mpdata_b200.adjoint as ma
+    faces, c0, rec, t_rec, rng = _c5_problem()
+    nsteps, every = 200, 20
+    shape = c0.shape
+
+    def lam_of(cN):
+        lam = np.zeros(c0.size)
+        np.add.at(lam, rec, 2.0 * (cN.reshape(-1)[rec] - t_rec))
+        return lam.reshape(shape)
+
+    def loss_of(cN):
+        return float(np.sum((cN.reshape(-1)[rec] - t_rec) ** 2))
+
+    def grad(a, c, dtype):
+        cN = a.forward(np.ascontiguousarray(c, dtype), nsteps).astype(np.float64)
+        return a.backward(np.ascontiguousarray(lam_of(cN), dtype)).astype(np.float64)
+
+    with ma.Adjoint(shape[2], shape[1], shape[0], order=2, dtype=np.float64,
+                    checkpoint_every=every, limiter=True) as a64:
+        a64.set_faces(*(np.ascontiguousarray(f, np.float64) for f in faces))
+        g64 = grad(a64, c0, np.float64)
+        cp = c0 * (1.0 + np.random.default_rng(11).uniform(-2.0 ** -24, 2.0 ** -24, shape))
+        sens = np.linalg.norm(grad(a64, cp, np.float64) - g64) / np.linalg.norm(g64)
+        errs = []
+        for _ in range(8):
+            v = rng.standard_normal(shape) * c0 * 1e-3
+            e = 1e-5
+            lp = loss_of(a64.forward(np.ascontiguousarray(c0 + e * v), nsteps))
+            lm = loss_of(a64.forward(np.ascontiguousarray(c0 - e * v), nsteps))
+            fd = (lp - lm) / (2 * e)
+            errs.append(abs(fd - float(np.sum(g64 * v))) / max(abs(fd), 1e-30))
+    assert float(np.median(errs)) <= 1e-5, errs
+    with ma.Adjoint(shape[2], shape[1], shape[0], order=2, dtype=np.float32,
+                    checkpoint_every=every, limiter=True) as a32:
+        a32.set_faces(*(np.ascontiguousarray(f, np.float32) for f in faces))
+        g32 = grad(a32, c0, np.float32)
+        cN = a32.forward(np.ascontiguousarray(c0, np.float32), nsteps).astype(np.float64)
+        lam = np.ascontiguousarray(lam_of(cN), np.float32)
+        g32b = a32.backward(lam).astype(np.float64)
+        g32c = a32.backward(lam).astype(np.float64)
+    rel32 = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
+    assert rel32 <= 0.1 and rel32 <= 3.0 * sens + 1e-6, (rel32, sens)
+    assert np.linalg.norm(g32b - g32c) / np.linalg.norm(g32b) <= 1e-5

@@ -98,3 +98,34 @@ def test_ensemble_autotune_picks_a_candidate_and_keeps_results():
                        5, 2, strict=True, limiter=True)
     assert np.array_equal(got, ref)
     assert got.min() >= 0.0
+
+
+@pytest.mark.parametrize("strict", [True, False], ids=["strict", "default"])
+def test_ensemble_matches_cpu_oracle_sample(strict):
+    """A sample of the benchmark-kind instances (rotation, Gaussian blob,
+    IORD 2 + limiter) against the CPU oracle on the 3-plane form directly:
+    strict arithmetic bit-identical, default within max-abs 1e-5."""
+    import oracle
+
+    import mpdata_b200 as m
+    cfg = workloads.ensemble(n=24, lo=64, hi=200, seed=17)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    steps = 6
+    with m.Ensemble([d["nx"] for d in cfg], [d["ny"] for d in cfg], order=2, limiter=True,
+                    strict=strict) as e:
+        for q, d in enumerate(cfg):
+            e.set_faces(q, f32(d["U"]), f32(d["V"]))
+            e.set_field(q, f32(d["c0"]))
+        e.step(steps)
+        got = {q: e.get_field(q) for q in (0, 5, 11, 23)}
+    for q, g in got.items():
+        d = cfg[q]
+        U = np.zeros((3, d["ny"], d["nx"]), np.float32); V = np.zeros_like(U)
+        U[1] = f32(d["U"]); V[1] = f32(d["V"])
+        c = np.repeat(f32(d["c0"])[None], 3, 0)
+        for _ in range(steps):
+            c = oracle.step_faces(U, V, np.zeros_like(U), c, 2, limiter=1)
+        if strict:
+            assert np.array_equal(g, c[1]), q
+        else:
+            assert float(np.abs(g - c[1]).max()) <= 1e-5, q

@@ -4,6 +4,9 @@ limiter, streamfunction flow): properties that do not depend on the size.
 * the headline arithmetic (two-cell pass, limiter, approx_div) leaves no
   negative cell and stays within relative L2 1e-5 of an FP64 run of the
   plain method after 10 steps;
+* with the y faces of the x = 1 column computed (vv_fix, the benchmark's
+  setting), every FP32 form stays within relative L2 1e-5 of the FP64 run
+  over the configuration's 100 steps;
 * a z-chunked march gives the same bits as the whole-column one at every
   chunk depth (chunks of 96 planes are the default here);
 * a grid of more than 2^31 elements per field steps correctly (64-bit
@@ -43,6 +46,19 @@ def _steps(m, wl, steps, dtype=np.float32, depth=None, **opts):
         return s.get_field(), mn, nneg
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("form", [dict(approx_div=True), dict(approx_div=True, precision_form=True),
+                                  dict()], ids=["approx_div", "precision_form", "plain"])
+def test_fullsize_100_steps_within_fp64_bound(m, wl, form):
+    """The throughput configuration over its own length (100 steps) with the
+    y faces of the x = 1 column computed (vv_fix): every FP32 form within
+    relative L2 1e-5 of the FP64 run, no negative cell."""
+    c64, _, _ = _steps(m, wl, 100, dtype=np.float64, vv_fix=True)
+    c32, mn, nneg = _steps(m, wl, 100, vv_fix=True, **form)
+    rel = np.linalg.norm(c32.astype(np.float64) - c64) / np.linalg.norm(c64)
+    assert rel <= REL_L2_BOUND, rel
+    assert nneg == 0 and mn >= 0.0
 
 
 def test_fullsize_positive_and_close_to_fp64(m, wl):

@@ -37,14 +37,15 @@ def _faces(case):
     return U.astype(np.float32), V.astype(np.float32), W.astype(np.float32)
 
 
-def _run(m, shape, order, opt, steps, approx=False, kernel=3, depth=None, seed=0):
+def _run(m, shape, order, opt, steps, approx=False, kernel=3, depth=None, seed=0,
+         precision_form=False):
     nx, ny, ns = shape
     case = workloads.random_case(nx, ny, ns, seed=seed)
     U, V, W = _faces(case)
     c = case["c0"].astype(np.float32)
     with m.Solver(nx, ny, ns, order=order, limiter=bool(opt.get("limiter")),
                   vv_fix=bool(opt.get("vv_fix")), div_mode=opt.get("div_mode", 0),
-                  approx_div=approx, kernel=kernel) as s:
+                  approx_div=approx, kernel=kernel, precision_form=precision_form) as s:
         if depth is not None:
             s.set_march_depth(depth)
         s.set_faces(U, V, W)
@@ -119,3 +120,30 @@ def test_pair_pass_against_fp64_run(m, approx):
         mn, nneg = s32.min()
     rel = np.linalg.norm(got - ref) / np.linalg.norm(ref)
     assert rel <= 1e-5 and nneg == 0, rel
+
+
+@pytest.mark.parametrize("approx", [False, True], ids=["ieee", "approx"])
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "x".join(map(str, s)))
+@pytest.mark.parametrize("order", [2, 3])
+def test_pair_precision_form_within_tolerance(m, approx, shape, order):
+    """The precision form on the two-cell pass (FP64 limiter sums and ratios)
+    against the oracle's precision form (wide_beta)."""
+    import oracle
+    opt = dict(limiter=1)
+    got, (U, V, W, c) = _run(m, shape, order, opt, 2, approx=approx, seed=sum(shape) + 3 * order,
+                             precision_form=True)
+    ref = c
+    for _ in range(2):
+        ref = oracle.step_faces(U, V, W, ref, order, limiter=1, wide_beta=1)
+    err = float(np.abs(got - ref).max())
+    assert err <= TOL, err
+
+
+@pytest.mark.parametrize("depth", [1, 5, 0])
+def test_pair_precision_form_z_chunks_bit_identical(m, depth):
+    shape = (70, 40, 26)
+    full, _ = _run(m, shape, 3, dict(limiter=1), 2, approx=True, depth=0, seed=9,
+                   precision_form=True)
+    got, _ = _run(m, shape, 3, dict(limiter=1), 2, approx=True, depth=depth, seed=9,
+                  precision_form=True)
+    assert np.array_equal(full, got)
