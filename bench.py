@@ -939,6 +939,13 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--ensemble-steps", type=int, default=500)
+    ap.add_argument("--acc-steps", type=int, default=None,
+                    help="horizon of the FP64 accuracy check (default: the configuration's "
+                         "100 steps; shorter only for profiling captures)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run only the adjoint configuration")
+    ap.add_argument("--adjoint-directions", type=int, default=32,
+                    help="finite-difference directions of the adjoint check")
     ap.add_argument("--ensemble-only", action="store_true",
                     help="run only the batched-ensemble configuration")
     ap.add_argument("--accuracy", action="store_true",
@@ -948,10 +955,19 @@ def main():
     args = ap.parse_args()
     if args.size:
         _set_size(*(int(v) for v in args.size.split(",")))
+    if args.acc_steps:
+        global ACC_STEPS
+        ACC_STEPS = args.acc_steps
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
     if args.accuracy:
         print(json.dumps(run_accuracy(args)), flush=True)
+        return
+    if args.adjoint_only:  # the adjoint configuration alone (profiling captures)
+        import torch
+        import mpdata_b200 as m
+        torch.cuda.set_device(0)
+        print(json.dumps(run_adjoint(m, torch, ndir=args.adjoint_directions)), flush=True)
         return
     if args.ensemble_only:  # the batched-ensemble configuration alone (profiling captures)
         import torch

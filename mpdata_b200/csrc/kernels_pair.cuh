@@ -29,8 +29,8 @@
 //    needs is the high face of a cell of the same CTA.
 //  * No divergent branches in the plane body: tile-edge threads select, and
 //    owned lanes are written by predicated scalar stores.
-//  * The precision form (WIDE): the limiter's in/out sums and its two ratios
-//    are formed in FP64 from the FP32 fluxes and rounded to FP32 once.
+//  * The precision form (WIDE): a limiter in/out sum near zero is formed
+//    again in FP64 from its flux parts and its ratio divided in FP64.
 //
 // Per plane k (limiter): [limited x/y faces of plane k-1, limited z face
 // k-3/2, donor fluxes, update of plane k-2; raw faces of plane k and z face
@@ -57,61 +57,14 @@ __host__ __device__ constexpr int stage_bytes() { return (SBX * SBY * 4 + 127) /
 // staged arrays: c, Uo, Vo, Wo (+ c^n with the limiter)
 template <bool LIM> __host__ __device__ constexpr int n_arrays() { return LIM ? 5 : 4; }
 template <bool LIM> __host__ __device__ constexpr int n_work() { return LIM ? 12 : 2; }
-constexpr int CL = kPairCL;  // CTAs per y-cluster of the limited march
 template <bool LIM> __host__ __device__ constexpr size_t smem_bytes()
 {
-    // + NSTAGE TMA barriers and the two neighbour-handshake barriers
     return (size_t)NSTAGE * n_arrays<LIM>() * stage_bytes() + (size_t)n_work<LIM>() * WPL * 4 +
-           (NSTAGE + 2) * 8;
+           NSTAGE * 8;
 }
 // Tile strides: cells of a CTA that are updated (x: 3..30 / 1..30, y: 2..CY-2 / 1..CY-1).
 template <bool LIM> __host__ __device__ constexpr int stride_x() { return LIM ? CX - 4 : CX - 2; }
 template <bool LIM> __host__ __device__ constexpr int stride_y() { return LIM ? CY - 3 : CY - 1; }
-
-// ---- y-clusters of the limited march ---------------------------------------
-// A cluster's CTAs are stacked in y (rank r holds rows r*CY .. r*CY + CY-1 of
-// the cluster).  Neighbours read each other's edge rows from distributed
-// shared memory: the low neighbour's raw y-face fluxes and donor fluxes of its
-// top row, the high neighbour's ratios of its bottom row.  Each phase ends
-// with a handshake: every CTA arrives on its neighbours' barrier and waits
-// (bounded) on its own, whose phase completes when all its neighbours have
-// arrived.
-__device__ __forceinline__ uint32_t cluster_map(const void* p, uint32_t rank)
-{
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(tma::smem_addr(p)), "r"(rank));
-    return r;
-}
-__device__ __forceinline__ float2 ld_remote2(uint32_t addr)
-{
-    float2 v;
-    asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
-    return v;
-}
-__device__ __forceinline__ void arrive_remote(uint32_t bar)
-{
-    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool wait_cluster(uint64_t* bar, uint32_t parity)
-{
-    for (uint32_t n = 0; n < tma::kWaitLimit; n++) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(tma::smem_addr(bar)), "r"(parity)
-            : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-// Every thread of every CTA of the cluster (kernel start and end only).
-__device__ __forceinline__ void cluster_sync_all()
-{
-    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
 
 // ---- paired arithmetic -----------------------------------------------------
 __device__ __forceinline__ float2 bc(float a) { return make_float2(a, a); }
@@ -373,8 +326,7 @@ struct PairSetup {
 };
 
 template <bool LIM, bool BORDER>
-__device__ __forceinline__ PairSetup pair_setup(const Dims& d, const PassArgs<float>& a, int i0, int j0,
-                                                int rank = 0)
+__device__ __forceinline__ PairSetup pair_setup(const Dims& d, const PassArgs<float>& a, int i0, int j0)
 {
     using namespace pair;
     PairSetup p;
@@ -388,9 +340,7 @@ __device__ __forceinline__ PairSetup pair_setup(const Dims& d, const PassArgs<fl
     p.iA = i0 + p.xA;
     p.j = j0 + ty;
     p.g = pair_geo(d, p.iA, p.j, a.vv_fix);
-    // with the limiter: two halo rows below the cluster, one above it
-    const int ox0 = LIM ? 3 : 1, ox1 = CX - 2;
-    const int oy0 = LIM ? (rank == 0 ? 2 : 0) : 1, oy1 = LIM ? (rank == CL - 1 ? CY - 2 : CY - 1) : CY - 1;
+    const int ox0 = LIM ? 3 : 1, ox1 = CX - 2, oy0 = LIM ? 2 : 1, oy1 = LIM ? CY - 2 : CY - 1;
     const bool own_y = ty >= oy0 && ty <= oy1;
     const bool inA = p.xA >= ox0 && p.xA <= ox1, inB = p.xA + 1 >= ox0 && p.xA + 1 <= ox1;
     p.ownA = own_y && inA && (!BORDER || p.g.cx);
@@ -554,7 +504,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                                                const CUtensorMap* map_c, const CUtensorMap* map_cn,
                                                const CUtensorMap* map_uo, const CUtensorMap* map_vo,
                                                const CUtensorMap* map_wo, unsigned char* smem,
-                                               int i0, int j0, int rank)
+                                               int i0, int j0)
 {
     using namespace pair;
     constexpr int NARR = n_arrays<true>();  // c, Uo, Vo, Wo, c^n
@@ -570,26 +520,16 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
     float* sDX = sBD + 2 * WPL;  // donor fluxes through the limited faces, two slots
     float* sDY = sDX + 2 * WPL;
     uint64_t* bars = reinterpret_cast<uint64_t*>(sDY + 2 * WPL);
-    uint64_t* nbar = bars + NSTAGE;  // neighbour handshakes after each phase (clusters)
-    const PairSetup p = pair_setup<true, BORDER>(d, a, i0, j0, rank);
+    const PairSetup p = pair_setup<true, BORDER>(d, a, i0, j0);
     const int ns = d.ns;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
     // The ring cells at x = 31 and y = CY-1 bound over a neighbour outside the
     // CTA: the edge threads take its c and c^n from the staged planes.
     const bool edge_x = tx == TX - 1, edge_y = ty == CY - 1;
-    // Cluster edges shared with a neighbour CTA: the bottom row of a CTA above
-    // rank 0 reads the low neighbour's top row; the top row of a CTA below the
-    // last rank reads the high neighbour's bottom row.
-    const bool nb_lo = CL > 1 && rank > 0, nb_hi = CL > 1 && rank < CL - 1;
-    const bool row_lo = nb_lo && ty == 0, row_hi = nb_hi && edge_y;
     const long long pp = d.pp;
 
     if (tid == 0) {
         for (int s = 0; s < NSTAGE; s++) tma::mbar_init(&bars[s], 1);
-        if (CL > 1) {
-            tma::mbar_init(&nbar[0], (nb_lo ? 1 : 0) + (nb_hi ? 1 : 0));
-            tma::mbar_init(&nbar[1], (nb_lo ? 1 : 0) + (nb_hi ? 1 : 0));
-        }
         tma::fence_barrier_init();
         tma::prefetch_map(map_c);
         tma::prefetch_map(map_cn);
@@ -597,35 +537,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
         tma::prefetch_map(map_vo);
         tma::prefetch_map(map_wo);
     }
-    // Neighbours' shared memory (same layout) and their handshake barriers.
-    uint32_t rem_lo = 0, rem_hi = 0;
-    if (CL > 1) {
-        if (nb_lo) rem_lo = cluster_map(smem, rank - 1);
-        if (nb_hi) rem_hi = cluster_map(smem, rank + 1);
-        cluster_sync_all();  // every CTA's barriers are initialised before any remote arrive
-    } else {
-        __syncthreads();
-    }
-    auto remote = [&](uint32_t base, const void* local) -> uint32_t {
-        return base + (uint32_t)(reinterpret_cast<const unsigned char*>(local) - smem);
-    };
-    uint32_t nb_phase = 0;  // parity of both handshake barriers (each completes once per plane)
-    // End of a phase: this CTA's shared-memory writes are done (and its reads
-    // of the neighbours' from the phase before); with clusters, also the
-    // neighbours'.
-    auto phase_sync = [&](int which) {
-        __syncthreads();
-        if (CL > 1) {
-            if (tid == 0) {
-                asm volatile("fence.acq_rel.cluster;" ::: "memory");
-                if (nb_lo) arrive_remote(remote(rem_lo, &nbar[which]));
-                if (nb_hi) arrive_remote(remote(rem_hi, &nbar[which]));
-                if (!wait_cluster(&nbar[which], nb_phase) && a.err) atomicOr(a.err, 2);
-            }
-            if (which == 1) nb_phase ^= 1;
-            __syncthreads();
-        }
-    };
+    __syncthreads();
     auto slot = [&](int s, int arr) -> const float* {
         return reinterpret_cast<const float*>(smem + (size_t)(s * NARR + arr) * SB);
     };
@@ -699,16 +611,12 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
             // a ratio plane is the first row of the next work array).
             {
                 const float buR = bu1[p.w + 2], bdR = bd1[p.w + 2];
-                float2 buU = ld2(bu1 + p.w + WX), bdU = ld2(bd1 + p.w + WX);
-                if (CL > 1 && row_hi) {  // ratios of the high neighbour's bottom row
-                    buU = ld_remote2(remote(rem_hi, bu1 + p.w - (CY - 1) * WX));
-                    bdU = ld_remote2(remote(rem_hi, bd1 + p.w - (CY - 1) * WX));
-                }
+                const float2 buU = ld2(bu1 + p.w + WX), bdU = ld2(bd1 + p.w + WX);
                 const float luy = limit(ru_prev.y, bu.y, bd.y, buR, bdR);
                 const float2 lvl = make_float2(limit(rv_prev.x, bu.x, bd.x, buU.x, bdU.x),
                                                limit(rv_prev.y, bu.y, bd.y, buU.y, bdU.y));
                 lu.y = edge_x ? ru_prev.y : luy;
-                lv = (edge_y && !nb_hi) ? rv_prev : lvl;
+                lv = edge_y ? rv_prev : lvl;
             }
             const float2 lw = make_float2(limit(rw_pp.x, bu2.x, bd2.x, bu.x, bd.x),
                                           limit(rw_pp.y, bu2.y, bd2.y, bu.y, bd.y));
@@ -739,10 +647,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 const float* dyp = sDY + PK * WPL;
                 const float2 dxo = ld2(dxp + p.w);
                 const float2 netx = make_float2(dxo.x - dxp[p.w - 1], dxo.y - dxo.x);
-                float2 dyl = ld2(dyp + p.w - WX);
-                if (CL > 1 && row_lo)  // donor flux through the low neighbour's top face
-                    dyl = ld_remote2(remote(rem_lo, dyp + p.w + (CY - 1) * WX));
-                const float2 nety = ld2(dyp + p.w) - dyl;
+                const float2 nety = ld2(dyp + p.w) - ld2(dyp + p.w - WX);
                 store_lanes(a.c_out + (q1 - pp), cq0 - ((netx + nety) + (dz - dz_prev)), p.ownA,
                             p.ownB);
             }
@@ -790,16 +695,14 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
             st2(sMX + p.w, mx0);
             st2(sMN + p.w, mn0);
         }
-        phase_sync(0);
+        __syncthreads();
 
         // ---- ratios of plane k ----
         {
             float2 bu = bc(1.f), bd = bc(1.f);
             if (kin) {
                 const float fxL = sFX[p.w - 1];
-                float2 fyL = ld2(sFY + p.w - WX);
-                if (CL > 1 && row_lo)  // raw flux through the low neighbour's top face
-                    fyL = ld_remote2(remote(rem_lo, sFY + p.w + (CY - 1) * WX));
+                const float2 fyL = ld2(sFY + p.w - WX);
                 const float2 fzL = flux2(rw_prev, cq1, cq2);  // raw z face k-1/2
                 // in: positive low-face and negative high-face fluxes; out: the rest
                 // (max(f,0) - f = max(-f,0)).  x lane-wise: A's faces are L|A and
@@ -826,45 +729,46 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 const float2 nU = edge_y ? min2(cU, cnU) : nUs;
                 float2 mx = make_float2(fmaxf(mAB, sMX[p.w - 1]), fmaxf(mAB, mR));
                 float2 mn = make_float2(fminf(nAB, sMN[p.w - 1]), fminf(nAB, nR));
-                float2 mD = ld2(sMX + p.w - WX), nD = ld2(sMN + p.w - WX);
-                if (CL > 1 && row_lo) {  // the row below lies in the staged planes
-                    const float2 cD = ld2(slot(S, 0) + p.o - Y), cnD = ld2(cnS + p.o - Y);
-                    mD = max2(cD, cnD);
-                    nD = min2(cD, cnD);
-                }
-                mx = max2(mx, max2(mD, mU));
-                mn = min2(mn, min2(nD, nU));
+                mx = max2(mx, max2(ld2(sMX + p.w - WX), mU));
+                mn = min2(mn, min2(ld2(sMN + p.w - WX), nU));
                 if (ns > 3) {
                     const float2 cnm = ld2(slot(SM1, 4) + p.o), cnp = ld2(slot(SP1, 4) + p.o);
                     mx = max2(mx, max2(max2(cq1, cnm), max2(cq3, cnp)));
                     mn = min2(mn, min2(min2(cq1, cnm), min2(cq3, cnp)));
                 }
+                const float2 fin = finx + ((py + pz) + ((hy - fyH) + (hz - fzH)));
+                const float2 fout = foutx + (((py - fyL) + (pz - fzL)) + (hy + hz));
+                const float2 eps = bc(FLT_MIN);
+                bu = min2(rat2<AP>(mx - cq2, fin + eps), bc(1.f));
+                bd = min2(rat2<AP>(cq2 - mn, fout + eps), bc(1.f));
                 if constexpr (WIDE) {
-                    // The precision form: the in/out sums (of the exact non-negative
-                    // flux parts) and the two ratios in FP64, rounded to FP32 once, so
-                    // a denominator near zero keeps its digits.
-                    const double finA = (((double)pL + (double)(pI - fxI)) +
-                                         ((double)py.x + (double)pz.x)) +
-                                        ((double)(hy.x - fyH.x) + (double)(hz.x - fzH.x));
-                    const double finB = (((double)pI + (double)(pH - fxH)) +
-                                         ((double)py.y + (double)pz.y)) +
-                                        ((double)(hy.y - fyH.y) + (double)(hz.y - fzH.y));
-                    const double foutA = (((double)(pL - fxL) + (double)pI) +
-                                          ((double)(py.x - fyL.x) + (double)(pz.x - fzL.x))) +
-                                         ((double)hy.x + (double)hz.x);
-                    const double foutB = (((double)(pI - fxI) + (double)pH) +
-                                          ((double)(py.y - fyL.y) + (double)(pz.y - fzL.y))) +
-                                         ((double)hy.y + (double)hz.y);
-                    bu = make_float2((float)fmin(((double)mx.x - (double)cq2.x) / (finA + DBL_MIN), 1.0),
-                                     (float)fmin(((double)mx.y - (double)cq2.y) / (finB + DBL_MIN), 1.0));
-                    bd = make_float2((float)fmin(((double)cq2.x - (double)mn.x) / (foutA + DBL_MIN), 1.0),
-                                     (float)fmin(((double)cq2.y - (double)mn.y) / (foutB + DBL_MIN), 1.0));
-                } else {
-                    const float2 fin = finx + ((py + pz) + ((hy - fyH) + (hz - fzH)));
-                    const float2 fout = foutx + (((py - fyL) + (pz - fzL)) + (hy + hz));
-                    const float2 eps = bc(FLT_MIN);
-                    bu = min2(rat2<AP>(mx - cq2, fin + eps), bc(1.f));
-                    bd = min2(rat2<AP>(cq2 - mn, fout + eps), bc(1.f));
+                    // The precision form: a sum near zero (below 2^-100, where FLT_MIN
+                    // and subnormal flux parts stop being negligible) is formed again
+                    // in FP64 from its exact non-negative parts and its ratio divided
+                    // in FP64, rounded to FP32 once.  Such sums are rare, so the branch
+                    // costs nothing where the field stays away from zero.
+                    constexpr float kNearZero = 0x1p-100f;
+                    if (fminf(fminf(fin.x, fin.y), fminf(fout.x, fout.y)) < kNearZero) {
+                        const double finA = (((double)pL + (double)(pI - fxI)) +
+                                             ((double)py.x + (double)pz.x)) +
+                                            ((double)(hy.x - fyH.x) + (double)(hz.x - fzH.x));
+                        const double finB = (((double)pI + (double)(pH - fxH)) +
+                                             ((double)py.y + (double)pz.y)) +
+                                            ((double)(hy.y - fyH.y) + (double)(hz.y - fzH.y));
+                        const double foutA = (((double)(pL - fxL) + (double)pI) +
+                                              ((double)(py.x - fyL.x) + (double)(pz.x - fzL.x))) +
+                                             ((double)hy.x + (double)hz.x);
+                        const double foutB = (((double)(pI - fxI) + (double)pH) +
+                                              ((double)(py.y - fyL.y) + (double)(pz.y - fzL.y))) +
+                                             ((double)hy.y + (double)hz.y);
+                        auto r64 = [](double n, double den) {
+                            return (float)fmin(n / (den + DBL_MIN), 1.0);
+                        };
+                        if (fin.x < kNearZero) bu.x = r64((double)mx.x - (double)cq2.x, finA);
+                        if (fin.y < kNearZero) bu.y = r64((double)mx.y - (double)cq2.y, finB);
+                        if (fout.x < kNearZero) bd.x = r64((double)cq2.x - (double)mn.x, foutA);
+                        if (fout.y < kNearZero) bd.y = r64((double)cq2.y - (double)mn.y, foutB);
+                    }
                 }
                 if constexpr (BORDER) {
                     bu = pick(p.g.cx, p.g.cy, bu, bc(1.f));
@@ -874,7 +778,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
             st2(sBU + PK * WPL + p.w, bu);
             st2(sBD + PK * WPL + p.w, bd);
         }
-        phase_sync(1);
+        __syncthreads();
         cq0 = cq1;
         cq1 = cq2;
         cq2 = cq3;
@@ -896,8 +800,6 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
         for (int pl = confirmed; pl <= issue_max; pl++)
             if (!tma::mbar_wait(&bars[pl & (NSTAGE - 1)], ((pl - kstart) / NSTAGE) & 1)) break;
     }
-    // no CTA leaves while a neighbour may still read its shared memory
-    if (CL > 1) cluster_sync_all();
 }
 
 template <bool LIM, bool AP, bool WIDE>
@@ -909,21 +811,17 @@ __global__ void __launch_bounds__(pair::NT, pair::NT >= 512 ? 1 : 2)
     using namespace pair;
     extern __shared__ __align__(128) unsigned char smem[];
     const int i0 = LIM ? stride_x<LIM>() * (int)blockIdx.x - 2 : stride_x<LIM>() * (int)blockIdx.x;
-    // with the limiter, y-clusters of CL CTAs (rank = position in the cluster)
-    // advance CL * CY - 3 rows
-    const int rank = LIM ? (int)blockIdx.y % CL : 0;
-    const int j0 = LIM ? (CL * CY - 3) * ((int)blockIdx.y / CL) - 1 + rank * CY
-                       : stride_y<LIM>() * (int)blockIdx.y;
+    const int j0 = LIM ? stride_y<LIM>() * (int)blockIdx.y - 1 : stride_y<LIM>() * (int)blockIdx.y;
     // CTAs whose every face is an interior face of the interior pattern take
     // the branch-free path (no boundary forms, no existence masks, no i = 1 column).
     const bool interior = i0 >= 2 && i0 + CX - 1 <= d.nx - 3 && j0 >= 1 && j0 + CY - 1 <= d.ny - 3;
     if constexpr (LIM) {
         if (interior)
             pair_march_lim<AP, WIDE, false>(d, a, &map_c, &map_cn, &map_uo, &map_vo, &map_wo, smem,
-                                            i0, j0, rank);
+                                            i0, j0);
         else
             pair_march_lim<AP, WIDE, true>(d, a, &map_c, &map_cn, &map_uo, &map_vo, &map_wo, smem,
-                                           i0, j0, rank);
+                                           i0, j0);
     } else {
         if (interior)
             pair_march_plain<AP, false>(d, a, &map_c, &map_uo, &map_vo, &map_wo, smem, i0, j0);
@@ -945,31 +843,12 @@ int launch_pair_variant(const Dims& d, const PassArgs<float>& a, cudaStream_t s)
     const int zb = a.zbase > 0 ? a.zbase : 1, ze = a.zend > 0 ? a.zend : d.ns - 1;
     if (ze <= zb) return 0;
     const int depth = a.zdepth > 0 ? a.zdepth : ze - zb;
-    const int rows = LIM ? CL * CY - 3 : stride_y<LIM>();  // rows a (cluster of) CTA(s) advances
-    const int cl = LIM ? CL : 1;
     dim3 g((d.nx - 2 + stride_x<LIM>() - 1) / stride_x<LIM>(),
-           cl * ((d.ny - 2 + rows - 1) / rows), (ze - zb + depth - 1) / depth);
+           (d.ny - 2 + stride_y<LIM>() - 1) / stride_y<LIM>(), (ze - zb + depth - 1) / depth);
     dim3 b(TX, CY);
     const CUtensorMap& cn = LIM ? *a.maps2.cn : *a.maps2.c;
-    if (cl == 1) {
-        k_pass_pair<LIM, AP, WIDE><<<g, b, smem, s>>>(d, a, *a.maps2.c, cn, *a.maps2.uo,
-                                                      *a.maps2.vo, *a.maps2.wo);
-        return 1;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = g;
-    cfg.blockDim = b;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 1;
-    attr[0].val.clusterDim.y = cl;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_pass_pair<LIM, AP, WIDE>, d, a, *a.maps2.c, cn, *a.maps2.uo,
-                       *a.maps2.vo, *a.maps2.wo);
+    k_pass_pair<LIM, AP, WIDE><<<g, b, smem, s>>>(d, a, *a.maps2.c, cn, *a.maps2.uo, *a.maps2.vo,
+                                                  *a.maps2.wo);
     return 1;
 }
 

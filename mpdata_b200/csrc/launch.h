@@ -35,16 +35,6 @@ constexpr int kBoxX = 40, kBoxY = 19;
 #endif
 constexpr int kPairCY = MPD_PAIR_CY;
 constexpr int kPairBoxX = 40, kPairBoxY = kPairCY + 2;
-// With the limiter, CTAs of the two-cell pass form clusters of kPairCL CTAs
-// stacked in y that take each other's edge rows (fluxes, ratios, donor
-// fluxes) from distributed shared memory instead of recomputing halo rows:
-// a cluster updates kPairCL * kPairCY - 3 rows.  1 = no clusters.
-#ifndef MPD_PAIR_CL
-#define MPD_PAIR_CL 1
-#endif
-constexpr int kPairCL = MPD_PAIR_CL;
-// Rows a cluster of limited two-cell CTAs advances in y.
-constexpr int pair_rows_per_cluster() { return kPairCL * kPairCY - 3; }
 
 // Per-pass description for the corrective-pass launchers.
 template <typename T> struct PassArgs {

@@ -174,12 +174,10 @@ int default_zdepth(const mpd::Solver* h)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
     const bool lim = h->opts.limiter != 0;
-    int sx, sy, per_sm, cl = 1;
+    int sx, sy, per_sm;
     if (h->pair) {
         sx = lim ? 28 : 30;
-        // with the limiter, clusters of kPairCL CTAs advance pair_rows_per_cluster() rows
-        sy = lim ? mpd::pair_rows_per_cluster() : mpd::kPairCY - 1;
-        cl = lim ? mpd::kPairCL : 1;
+        sy = lim ? mpd::kPairCY - 3 : mpd::kPairCY - 1;
         per_sm = mpd::kPairCY >= 32 ? 1 : 2;
     } else {
         sx = lim ? 30 : 32;
@@ -187,7 +185,7 @@ int default_zdepth(const mpd::Solver* h)
         per_sm = 2;
     }
     const long long bx = (h->d.nx - 2 + sx - 1) / sx;
-    const long long by = cl * ((h->d.ny - 2 + sy - 1) / sy);
+    const long long by = (h->d.ny - 2 + sy - 1) / sy;
     const long long want = 6LL * per_sm * sms;
     const int interior = h->d.ns - 2;
     long long chunks = (want + bx * by - 1) / (bx * by);

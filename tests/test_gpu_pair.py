@@ -147,3 +147,30 @@ def test_pair_precision_form_z_chunks_bit_identical(m, depth):
     got, _ = _run(m, shape, 3, dict(limiter=1), 2, approx=True, depth=depth, seed=9,
                   precision_form=True)
     assert np.array_equal(full, got)
+
+
+@pytest.mark.parametrize("approx", [False, True], ids=["ieee", "approx"])
+def test_pair_precision_form_near_zero_fields(m, approx):
+    """A field spanning 1 down to subnormal values, with exact zeros, so that
+    limiter sums fall below 2^-100 and take the precision form's FP64 path:
+    the result stays finite, non-negative and within max-abs 1e-5 of the
+    oracle's precision form."""
+    import oracle
+    nx, ny, ns = 70, 40, 12
+    case = workloads.random_case(nx, ny, ns, seed=31)
+    U, V, W = _faces(case)
+    rng = np.random.default_rng(32)
+    c = (rng.uniform(0.0, 1.0, (ns, ny, nx)) * 10.0 ** rng.integers(-44, 1, (ns, ny, nx)))
+    c[rng.random(c.shape) < 0.2] = 0.0
+    c = c.astype(np.float32)
+    with m.Solver(nx, ny, ns, order=2, limiter=True, approx_div=approx, kernel=3,
+                  precision_form=True) as s:
+        s.set_faces(U, V, W)
+        s.set_field(c)
+        s.step(2)
+        got = s.get_field()
+    ref = c
+    for _ in range(2):
+        ref = oracle.step_faces(U, V, W, ref, 2, limiter=1, wide_beta=1)
+    assert np.isfinite(got).all() and float(got.min()) >= 0.0
+    assert float(np.abs(got - ref).max()) <= TOL
