@@ -29,8 +29,9 @@
 //    needs is the high face of a cell of the same CTA.
 //  * No divergent branches in the plane body: tile-edge threads select, and
 //    owned lanes are written by predicated scalar stores.
-//  * The precision form (WIDE): a limiter in/out sum near zero is formed
-//    again in FP64 from its flux parts and its ratio divided in FP64.
+//  * The precision form (WIDE): a non-zero limiter in/out sum near zero is
+//    formed again in FP64 from its flux parts and its ratio divided in FP64;
+//    every ratio is shrunk by 2^-20 so rounding cannot break positivity.
 //
 // Per plane k (limiter): [limited x/y faces of plane k-1, limited z face
 // k-3/2, donor fluxes, update of plane k-2; raw faces of plane k and z face
@@ -739,16 +740,28 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 const float2 fin = finx + ((py + pz) + ((hy - fyH) + (hz - fzH)));
                 const float2 fout = foutx + (((py - fyL) + (pz - fzL)) + (hy + hz));
                 const float2 eps = bc(FLT_MIN);
-                bu = min2(rat2<AP>(mx - cq2, fin + eps), bc(1.f));
-                bd = min2(rat2<AP>(cq2 - mn, fout + eps), bc(1.f));
+                // The precision form shrinks every ratio by 2^-20 before the clamp:
+                // the rounding of the ratio (<= 2 ulp with rcp.approx), of the
+                // limited fluxes and of their sums then never lets a cell's
+                // limited out-fluxes exceed its margin above its lower bound, so a
+                // field with zeros stays non-negative.
+                float2 rup = rat2<AP>(mx - cq2, fin + eps), rdn = rat2<AP>(cq2 - mn, fout + eps);
                 if constexpr (WIDE) {
-                    // The precision form: a sum near zero (below 2^-100, where FLT_MIN
-                    // and subnormal flux parts stop being negligible) is formed again
-                    // in FP64 from its exact non-negative parts and its ratio divided
-                    // in FP64, rounded to FP32 once.  Such sums are rare, so the branch
-                    // costs nothing where the field stays away from zero.
+                    rup = rup * bc(1.f - 0x1p-20f);
+                    rdn = rdn * bc(1.f - 0x1p-20f);
+                }
+                bu = min2(rup, bc(1.f));
+                bd = min2(rdn, bc(1.f));
+                if constexpr (WIDE) {
+                    // A non-zero sum near zero (below 2^-100, where FLT_MIN and
+                    // subnormal flux parts stop being negligible) is formed again in
+                    // FP64 from its exact non-negative parts and its ratio divided in
+                    // FP64.  A zero sum needs nothing: no flux of that direction is
+                    // limited by it.  Such sums are rare, so the branch costs nothing
+                    // where the field stays away from zero.
                     constexpr float kNearZero = 0x1p-100f;
-                    if (fminf(fminf(fin.x, fin.y), fminf(fout.x, fout.y)) < kNearZero) {
+                    auto near0 = [&](float v) { return v > 0.f && v < kNearZero; };
+                    if (near0(fin.x) || near0(fin.y) || near0(fout.x) || near0(fout.y)) {
                         const double finA = (((double)pL + (double)(pI - fxI)) +
                                              ((double)py.x + (double)pz.x)) +
                                             ((double)(hy.x - fyH.x) + (double)(hz.x - fzH.x));
@@ -762,12 +775,12 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                                               ((double)(py.y - fyL.y) + (double)(pz.y - fzL.y))) +
                                              ((double)hy.y + (double)hz.y);
                         auto r64 = [](double n, double den) {
-                            return (float)fmin(n / (den + DBL_MIN), 1.0);
+                            return (float)fmin(n / (den + DBL_MIN) * (1.0 - 0x1p-20), 1.0);
                         };
-                        if (fin.x < kNearZero) bu.x = r64((double)mx.x - (double)cq2.x, finA);
-                        if (fin.y < kNearZero) bu.y = r64((double)mx.y - (double)cq2.y, finB);
-                        if (fout.x < kNearZero) bd.x = r64((double)cq2.x - (double)mn.x, foutA);
-                        if (fout.y < kNearZero) bd.y = r64((double)cq2.y - (double)mn.y, foutB);
+                        if (near0(fin.x)) bu.x = r64((double)mx.x - (double)cq2.x, finA);
+                        if (near0(fin.y)) bu.y = r64((double)mx.y - (double)cq2.y, finB);
+                        if (near0(fout.x)) bd.x = r64((double)cq2.x - (double)mn.x, foutA);
+                        if (near0(fout.y)) bd.y = r64((double)cq2.y - (double)mn.y, foutB);
                     }
                 }
                 if constexpr (BORDER) {
