@@ -492,7 +492,7 @@ def run_ensemble(m, torch, steps: int, base_steps: int):
     cells = sum((a - 2) * (b - 2) for a, b in zip(nx, ny))
     stream = torch.cuda.Stream()  # graph capture needs a non-default stream
     f32 = lambda a: np.ascontiguousarray(a, np.float32)
-    e = m.Ensemble(nx, ny, order=2, limiter=True)
+    e = m.Ensemble(nx, ny, order=2, limiter=True, approx_div=True)
     e.set_stream(stream.cuda_stream)
     for q, d in enumerate(cfg):
         e.set_faces(q, f32(d["U"]), f32(d["V"]))
@@ -516,7 +516,7 @@ def run_ensemble(m, torch, steps: int, base_steps: int):
     # per-instance baseline
     solvers = []
     for d in cfg:
-        s = m.Solver(d["nx"], d["ny"], 3, order=2, limiter=True)
+        s = m.Solver(d["nx"], d["ny"], 3, order=2, limiter=True, approx_div=True)
         s.set_stream(stream.cuda_stream)
         U = np.zeros((3, d["ny"], d["nx"]), np.float32); V = np.zeros_like(U)
         U[1] = d["U"]; V[1] = d["V"]
@@ -595,7 +595,7 @@ def run_adjoint(m, torch, nsteps: int = 200, every: int = 20, ndir: int = 32):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     stream = torch.cuda.current_stream()
-    grads = {}
+    grads, fwd = {}, {}
     for dt in (np.float32, np.float64):
         a = ma.Adjoint(n, n, ns, order=2, dtype=dt, checkpoint_every=every, limiter=True)
         a.set_stream(stream.cuda_stream)
@@ -607,6 +607,7 @@ def run_adjoint(m, torch, nsteps: int = 200, every: int = 20, ndir: int = 32):
         ev1.record(stream)
         ev1.synchronize()
         t_f = ev0.elapsed_time(ev1)
+        fwd[np.dtype(dt).name] = cN.astype(np.float64)
         lam = np.ascontiguousarray(lam_of(cN.astype(np.float64)), dt)
         ev0.record(stream)
         g = a.backward(lam)
@@ -623,13 +624,18 @@ def run_adjoint(m, torch, nsteps: int = 200, every: int = 20, ndir: int = 32):
             out["fp32_adjoint_run_to_run_rel_l2"] = float(
                 np.linalg.norm(g2 - grads["float32"]) / np.linalg.norm(grads["float32"]))
         else:
-            # the FP64 adjoint's own sensitivity: the same window from c0
-            # perturbed by half an FP32 ulp per cell (one rounding to FP32)
-            cp = half_ulp_perturbed(c0)
-            cNp = a.forward(np.ascontiguousarray(cp), nsteps)
-            gp = a.backward(np.ascontiguousarray(lam_of(cNp))).astype(np.float64)
-            out["fp64_adjoint_half_ulp_sensitivity_rel_l2"] = float(
-                np.linalg.norm(gp - grads["float64"]) / np.linalg.norm(grads["float64"]))
+            # the FP64 adjoint's own sensitivity: the same window (same seed
+            # lambda) from c0 perturbed per cell by half an FP32 ulp (one
+            # rounding) and by 2^-20 (the FP32 forward's distance from the FP64
+            # one after the 200 steps)
+            lam64 = np.ascontiguousarray(lam_of(cN.astype(np.float64)))
+            for key, amp in (("half_ulp", 2.0 ** -24), ("2^-20", 2.0 ** -20)):
+                rng_p = np.random.default_rng(11)
+                cp = c0 * (1.0 + rng_p.uniform(-amp, amp, c0.shape))
+                a.forward(np.ascontiguousarray(cp), nsteps)
+                gp = a.backward(lam64).astype(np.float64)
+                out[f"fp64_adjoint_sensitivity_{key}_rel_l2"] = float(
+                    np.linalg.norm(gp - grads["float64"]) / np.linalg.norm(grads["float64"]))
         a.close()
     # production forward step (fused kernels) on the same problem
     s = m.Solver(n, n, ns, order=2, limiter=True)
@@ -647,6 +653,8 @@ def run_adjoint(m, torch, nsteps: int = 200, every: int = 20, ndir: int = 32):
     out["t_adj_over_t_fwd_recording"] = out["t_adj_ms_per_step"] / out["t_fwd_recording_ms_per_step"]
     g32, g64 = grads["float32"], grads["float64"]
     out["fp32_vs_fp64_adjoint_rel_l2"] = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+    out["fp32_vs_fp64_forward_rel_l2"] = float(
+        np.linalg.norm(fwd["float32"] - fwd["float64"]) / np.linalg.norm(fwd["float64"]))
     # central differences of the FP64 window along random directions
     a64 = ma.Adjoint(n, n, ns, order=2, dtype=np.float64, checkpoint_every=every, limiter=True)
     a64.set_faces(*(np.ascontiguousarray(f, np.float64) for f in faces))

@@ -43,13 +43,14 @@ template <typename T> __device__ __forceinline__ Nb2<T> gather2(const T* c, cons
 }
 
 // x face between i and i+1 (uu.c:18-102 with the z terms, all zero here, dropped).
-template <bool AP, typename T>
+// BORDER = false: the caller knows the face takes the interior pattern.
+template <bool AP, bool BORDER, typename T>
 __device__ __forceinline__ T face_u2(const Nb2<T>& n, int i, int nx, int use_div)
 {
     T vb, neg_div = T(0);
-    if (i == 0) {
+    if (BORDER && i == 0) {
         vb = T(0.5) * (n.vRD + n.vR);
-    } else if (i == nx - 2) {
+    } else if (BORDER && i == nx - 2) {
         vb = T(0.5) * (n.vD + n.v);
     } else {
         vb = T(0.25) * (((n.vRD + n.vR) + n.v) + n.vD);
@@ -72,21 +73,21 @@ __device__ __forceinline__ T face_u2(const Nb2<T>& n, int i, int nx, int use_div
 }
 
 // y face between j and j+1 (vv.c:21-107, z terms dropped, column rule kept).
-template <bool AP, typename T>
+template <bool AP, bool BORDER, typename T>
 __device__ __forceinline__ T face_v2(const Nb2<T>& n, int i, int j, int ny, int use_div, int vv_fix,
                                     int pass, T vadv)
 {
     T ub, neg_div = T(0);
-    if (j == 0) {
+    if (BORDER && j == 0) {
         ub = T(0.5) * (n.uLU + n.uU);
-    } else if (j == ny - 2) {
+    } else if (BORDER && j == ny - 2) {
         ub = T(0.5) * (n.uL + n.u);
     } else {
-        if (i == 1 && !vv_fix) return (pass & 1) ? T(0) : vadv;  // vv.c:81-82
+        if (BORDER && i == 1 && !vv_fix) return (pass & 1) ? T(0) : vadv;  // vv.c:81-82
         ub = T(0.25) * (((n.uLU + n.uU) + n.u) + n.uL);
         if (use_div) {
-            const T ul2u = (i >= 2) ? n.uL2U : T(0);
-            const T ul2 = (i >= 2) ? n.uL2 : T(0);
+            const T ul2u = (!BORDER || i >= 2) ? n.uL2U : T(0);
+            const T ul2 = (!BORDER || i >= 2) ? n.uL2 : T(0);
             T s = n.vU - n.vD;
             s = s + n.uLU;
             s = s - ul2u;
@@ -227,85 +228,95 @@ __global__ void __launch_bounds__(TX * TY)
         const T* vadv = arena + in.f[0][1];
         const int rx = (i0 - H) - ((i0 - H) & ~(V - 1));  // alignment slack of this tile
         const int o = (y + H) * SX + (x + H) + rx;
-        if constexpr (FUSE0) {
-            // c^(1) over local [-1, TX] x [-1, TY] (every cell the pass reads):
-            // the donor update of interior cells, the fixed shell copied, 0 outside
-            T* c1 = bC[0];
-            for (int e = tid; e < (TX + 2) * (TY + 2); e += NT) {
-                const int ly = e / (TX + 2) - 1, lx = e - (ly + 1) * (TX + 2) - 1;
-                const int q = (ly + H) * SX + (lx + H) + rx;
-                const int gi = i0 + lx, gj = j0 + ly;
-                T v = sN[q];
-                if (gi >= 1 && gi <= nx - 2 && gj >= 1 && gj <= ny - 2) {
-                    const T cc = sN[q];
-                    const T fx = upwind(cc, sN[q + 1], sU[q]) - upwind(sN[q - 1], cc, sU[q - 1]);
-                    const T fy = upwind(cc, sN[q + SX], sV[q]) - upwind(sN[q - SX], cc, sV[q - SX]);
-                    v = cc - T(0.5) * (fx + fy);
+        // Tiles whose every cell, face and c^(1) cell takes the interior forms
+        // run a copy without the boundary cases (uniform over the CTA).
+        auto item_body = [&](auto border_tag) {
+            constexpr bool BORDER = decltype(border_tag)::value;
+            if constexpr (FUSE0) {
+                // c^(1) over local [-1, TX] x [-1, TY] (every cell the pass reads):
+                // the donor update of interior cells, the fixed shell copied, 0 outside
+                T* c1 = bC[0];
+                for (int e = tid; e < (TX + 2) * (TY + 2); e += NT) {
+                    const int ly = e / (TX + 2) - 1, lx = e - (ly + 1) * (TX + 2) - 1;
+                    const int q = (ly + H) * SX + (lx + H) + rx;
+                    const int gi = i0 + lx, gj = j0 + ly;
+                    T v = sN[q];
+                    if (!BORDER || (gi >= 1 && gi <= nx - 2 && gj >= 1 && gj <= ny - 2)) {
+                        const T cc = sN[q];
+                        const T fx = upwind(cc, sN[q + 1], sU[q]) - upwind(sN[q - 1], cc, sU[q - 1]);
+                        const T fy = upwind(cc, sN[q + SX], sV[q]) - upwind(sN[q - SX], cc, sV[q - SX]);
+                        v = cc - T(0.5) * (fx + fy);
+                    }
+                    c1[q] = v;
                 }
-                c1[q] = v;
+                __syncthreads();
             }
-            __syncthreads();
-        }
 
-        const int i = i0 + x, j = j0 + y;
-        const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
-        const bool owned = cell_in && x >= LO && x <= TX - 1 - HI && y >= LO && y <= TY - 1 - HI;
-        T ru = T(0), rv = T(0);
-        {
-            const Nb2<T> nb = gather2(sC, sU, sV, o, SX);
-            if (i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2) ru = face_u2<AP>(nb, i, nx, p.use_div);
-            if (i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2) {
-                const T va = (i == 1) ? vadv[(long long)j * px + 1] : T(0);
-                rv = face_v2<AP>(nb, i, j, ny, p.use_div, p.vv_fix, p.pass, va);
+            const int i = i0 + x, j = j0 + y;
+            const bool cell_in = !BORDER || (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2);
+            const bool owned = cell_in && x >= LO && x <= TX - 1 - HI && y >= LO && y <= TY - 1 - HI;
+            T ru = T(0), rv = T(0);
+            {
+                const Nb2<T> nb = gather2(sC, sU, sV, o, SX);
+                if (!BORDER || (i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2))
+                    ru = face_u2<AP, BORDER>(nb, i, nx, p.use_div);
+                if (!BORDER || (i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2)) {
+                    const T va = (BORDER && i == 1) ? vadv[(long long)j * px + 1] : T(0);
+                    rv = face_v2<AP, BORDER>(nb, i, j, ny, p.use_div, p.vv_fix, p.pass, va);
+                }
             }
-        }
-        sRU[w] = ru;
-        sRV[w] = rv;
-        __syncthreads();
-
-        T ur = ru, ul = sRU[w - 1], vt = rv, vb = sRV[w - WX];
-        if (LIM) {
-            T bu = T(1), bd = T(1);
-            if (cell_in) {
-                const T psi = sC[o], cl = sC[o - 1], cr = sC[o + 1], cd = sC[o - SX], cu = sC[o + SX];
-                T mx = vmax(psi, sN[o]), mn = vmin(psi, sN[o]);
-                mx = vmax(vmax(cl, sN[o - 1]), mx); mn = vmin(vmin(cl, sN[o - 1]), mn);
-                mx = vmax(vmax(cr, sN[o + 1]), mx); mn = vmin(vmin(cr, sN[o + 1]), mn);
-                mx = vmax(vmax(cd, sN[o - SX]), mx); mn = vmin(vmin(cd, sN[o - SX]), mn);
-                mx = vmax(vmax(cu, sN[o + SX]), mx); mn = vmin(vmin(cu, sN[o + SX]), mn);
-                A fin = A(0), fout = A(0);
-                lim_acc(lim_flux<T, A>(ul, cl, psi), false, fin, fout);
-                lim_acc(lim_flux<T, A>(ru, psi, cr), true, fin, fout);
-                lim_acc(lim_flux<T, A>(vb, cd, psi), false, fin, fout);
-                lim_acc(lim_flux<T, A>(rv, psi, cu), true, fin, fout);
-                bu = T(ratio<AP>(A(mx) - A(psi), fin + lim_tiny<A>()));
-                bd = T(ratio<AP>(A(psi) - A(mn), fout + lim_tiny<A>()));
-            }
-            sBU[w] = bu;
-            sBD[w] = bd;
+            sRU[w] = ru;
+            sRV[w] = rv;
             __syncthreads();
-            auto BU = [&](int q2) { return sBU[q2]; };
-            auto BD = [&](int q2) { return sBD[q2]; };
+
+            T ur = ru, ul = sRU[w - 1], vt = rv, vb = sRV[w - WX];
+            if (LIM) {
+                T bu = T(1), bd = T(1);
+                if (cell_in) {
+                    const T psi = sC[o], cl = sC[o - 1], cr = sC[o + 1], cd = sC[o - SX], cu = sC[o + SX];
+                    T mx = vmax(psi, sN[o]), mn = vmin(psi, sN[o]);
+                    mx = vmax(vmax(cl, sN[o - 1]), mx); mn = vmin(vmin(cl, sN[o - 1]), mn);
+                    mx = vmax(vmax(cr, sN[o + 1]), mx); mn = vmin(vmin(cr, sN[o + 1]), mn);
+                    mx = vmax(vmax(cd, sN[o - SX]), mx); mn = vmin(vmin(cd, sN[o - SX]), mn);
+                    mx = vmax(vmax(cu, sN[o + SX]), mx); mn = vmin(vmin(cu, sN[o + SX]), mn);
+                    A fin = A(0), fout = A(0);
+                    lim_acc(lim_flux<T, A>(ul, cl, psi), false, fin, fout);
+                    lim_acc(lim_flux<T, A>(ru, psi, cr), true, fin, fout);
+                    lim_acc(lim_flux<T, A>(vb, cd, psi), false, fin, fout);
+                    lim_acc(lim_flux<T, A>(rv, psi, cu), true, fin, fout);
+                    bu = T(ratio<AP>(A(mx) - A(psi), fin + lim_tiny<A>()));
+                    bd = T(ratio<AP>(A(psi) - A(mn), fout + lim_tiny<A>()));
+                }
+                sBU[w] = bu;
+                sBD[w] = bd;
+                __syncthreads();
+                auto BU = [&](int q2) { return sBU[q2]; };
+                auto BD = [&](int q2) { return sBD[q2]; };
+                if (owned) {
+                    ur = limit_face(ru, BU(w), BD(w), BU(w + 1), BD(w + 1));
+                    ul = limit_face(ul, BU(w - 1), BD(w - 1), BU(w), BD(w));
+                    vt = limit_face(rv, BU(w), BD(w), BU(w + WX), BD(w + WX));
+                    vb = limit_face(vb, BU(w - WX), BD(w - WX), BU(w), BD(w));
+                }
+            }
             if (owned) {
-                ur = limit_face(ru, BU(w), BD(w), BU(w + 1), BD(w + 1));
-                ul = limit_face(ul, BU(w - 1), BD(w - 1), BU(w), BD(w));
-                vt = limit_face(rv, BU(w), BD(w), BU(w + WX), BD(w + WX));
-                vb = limit_face(vb, BU(w - WX), BD(w - WX), BU(w), BD(w));
+                const long long q = (long long)j * px + i;
+                const T cc = sC[o];
+                const T fx = upwind(cc, sC[o + 1], ur) - upwind(sC[o - 1], cc, ul);
+                const T fy = upwind(cc, sC[o + SX], vt) - upwind(sC[o - SX], cc, vb);
+                arena[in.c[p.out] + q] = cc - T(0.5) * (fx + fy);
+                if (p.write_faces) {
+                    arena[in.f[p.ws][0] + q] = ur;
+                    arena[in.f[p.ws][1] + q] = vt;
+                    if (BORDER && i == 1) arena[in.f[p.ws][0] + q - 1] = ul;
+                    if (BORDER && j == 1) arena[in.f[p.ws][1] + q - px] = vb;
+                }
             }
-        }
-        if (owned) {
-            const long long q = (long long)j * px + i;
-            const T cc = sC[o];
-            const T fx = upwind(cc, sC[o + 1], ur) - upwind(sC[o - 1], cc, ul);
-            const T fy = upwind(cc, sC[o + SX], vt) - upwind(sC[o - SX], cc, vb);
-            arena[in.c[p.out] + q] = cc - T(0.5) * (fx + fy);
-            if (p.write_faces) {
-                arena[in.f[p.ws][0] + q] = ur;
-                arena[in.f[p.ws][1] + q] = vt;
-                if (i == 1) arena[in.f[p.ws][0] + q - 1] = ul;
-                if (j == 1) arena[in.f[p.ws][1] + q - px] = vb;
-            }
-        }
+        };
+        if (i0 >= 2 && i0 + TX <= nx - 2 && j0 >= 2 && j0 + TY <= ny - 2)
+            item_body(std::false_type{});
+        else
+            item_body(std::true_type{});
         __syncthreads();  // every read of this buffer is done before it is refilled
     }
 }

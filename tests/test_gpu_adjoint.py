@@ -163,8 +163,9 @@ def test_c5_window_adjoint():
     * FP64 adjoint against FP64 central differences along 8 random
       directions: median relative error <= 1e-5;
     * FP32 adjoint against the FP64 adjoint: relative L2 <= 0.1 and no more
-      than 3x the FP64 adjoint's own change when c0 moves by half an FP32 ulp
-      per cell (the limiter's selections move with the rounding);
+      than 4x the FP64 adjoint's own change when c0 moves by 2^-20 per cell
+      (relative), the size by which the FP32 forward leaves the FP64 one over
+      the window (the limiter's frozen selections move with the trajectory);
     * two FP32 reverse sweeps of the same window agree to relative L2 1e-5
       (the scatter-adds are atomic, so their summation order varies)."""
     import mpdata_b200.adjoint as ma
@@ -188,8 +189,9 @@ def test_c5_window_adjoint():
                     checkpoint_every=every, limiter=True) as a64:
         a64.set_faces(*(np.ascontiguousarray(f, np.float64) for f in faces))
         g64 = grad(a64, c0, np.float64)
-        cp = c0 * (1.0 + np.random.default_rng(11).uniform(-2.0 ** -24, 2.0 ** -24, shape))
+        cp = c0 * (1.0 + np.random.default_rng(11).uniform(-2.0 ** -20, 2.0 ** -20, shape))
         sens = np.linalg.norm(grad(a64, cp, np.float64) - g64) / np.linalg.norm(g64)
+        c64 = a64.forward(np.ascontiguousarray(c0), nsteps)
         errs = []
         for _ in range(8):
             v = rng.standard_normal(shape) * c0 * 1e-3
@@ -204,9 +206,11 @@ def test_c5_window_adjoint():
         a32.set_faces(*(np.ascontiguousarray(f, np.float32) for f in faces))
         g32 = grad(a32, c0, np.float32)
         cN = a32.forward(np.ascontiguousarray(c0, np.float32), nsteps).astype(np.float64)
+        # the FP32 window leaves the FP64 one by about the perturbation above
+        assert np.linalg.norm(cN - c64) / np.linalg.norm(c64) <= 4e-6
         lam = np.ascontiguousarray(lam_of(cN), np.float32)
         g32b = a32.backward(lam).astype(np.float64)
         g32c = a32.backward(lam).astype(np.float64)
     rel32 = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
-    assert rel32 <= 0.1 and rel32 <= 3.0 * sens + 1e-6, (rel32, sens)
+    assert rel32 <= 0.1 and rel32 <= 4.0 * sens + 1e-6, (rel32, sens)
     assert np.linalg.norm(g32b - g32c) / np.linalg.norm(g32b) <= 1e-5
