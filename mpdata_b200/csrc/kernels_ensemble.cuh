@@ -12,10 +12,13 @@
 // The corrective pass stages each item's tile with a halo of 3 into shared
 // memory by 16-byte cp.async chunks (rows rounded down to a 16-byte
 // boundary), double-buffered (the next item's copies run while the current
-// item computes); the first corrective pass forms c^(1) itself (FUSE0), forms the faces of every cell of the tile (and,
-// with the limiter, their ratios) and updates the cells it owns: all but the
-// first column and row (the first two and the last with the limiter), so
-// every face an owned cell reads is the high face of a tile cell.  Tile shape
+// item computes; four barriers per item).  The first corrective pass forms
+// c^(1) itself from c^n and the advective faces (FUSE0, no pass-0 launch).
+// Each pass forms the faces of every cell of the tile (and, with the limiter,
+// their ratios) and updates the cells it owns: all but the first column and
+// row (the first two and the last with the limiter), so every face an owned
+// cell reads is the high face of a tile cell.  Tiles away from the instance's
+// boundary run a copy without the boundary cases.  Tile shape
 // TX x TY is a template parameter chosen by the host-side autotuner.
 //
 // Included by kernels_all.cuh inside namespace mpd::MPD_NS.
@@ -210,13 +213,12 @@ __global__ void __launch_bounds__(TX * TY)
     int b = 0;
     if ((int)blockIdx.x < nitems) stage(blockIdx.x, 0);
     for (int it = blockIdx.x; it < nitems; it += gridDim.x, b ^= 1) {
-        if (it + (int)gridDim.x < nitems) {  // the next item's tile into the other buffer
-            stage(it + gridDim.x, b ^ 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();  // this item's tile has landed for every thread
+        cp_async_wait<0>();  // this item's tile (the only copy group in flight)
+        // ...has landed for every thread, and every thread is done with the
+        // previous item, so its buffers (the other stage, c^(1), the work
+        // planes) may be refilled
+        __syncthreads();
+        if (it + (int)gridDim.x < nitems) stage(it + gridDim.x, b ^ 1);  // overlaps this item
         const T* sC = bC[FUSE0 ? 0 : b];
         const T* sU = bU[b];
         const T* sV = bV[b];
@@ -317,7 +319,6 @@ __global__ void __launch_bounds__(TX * TY)
             item_body(std::false_type{});
         else
             item_body(std::true_type{});
-        __syncthreads();  // every read of this buffer is done before it is refilled
     }
 }
 
