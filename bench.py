@@ -480,8 +480,10 @@ def run_gpu(args):
 
 def run_ensemble(m, torch, steps: int, base_steps: int):
     """Batched-ensemble configuration: 256 independent 2D instances (NX, NY in
-    [64, 512]), IORD 2 + limiter, FP32, one persistent launch per pass replayed
-    as a CUDA graph with the autotuned tile shape; against the same instances
+    [64, 512]), IORD 2 + limiter, FP32 with hardware-reciprocal ratios (the
+    headline form), one persistent launch per step (pass 0 formed inside the
+    corrective pass) replayed as a CUDA graph with the autotuned tile shape,
+    clocks sampled over the timed region; against the same instances
     stepped one after another through per-instance solvers (nx x ny x 3 form,
     256 sequential solver steps per ensemble step).  Both timed with CUDA
     events on one stream."""
@@ -506,10 +508,13 @@ def run_ensemble(m, torch, steps: int, base_steps: int):
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
     e0.record(stream)
     e.step(steps)
     e1.record(stream)
     e1.synchronize()
+    clk = clocks.stop()
     t_ens = e0.elapsed_time(e1)
     mins = [float(e.get_field(q)[1:-1, 1:-1].min()) for q in range(len(cfg))]
     e.close()
@@ -546,6 +551,7 @@ def run_ensemble(m, torch, steps: int, base_steps: int):
                            "ms_per_step": t_seq / base_steps,
                            "how": "256 per-instance solvers (nx x ny x 3), stepped one after another"},
             "speedup_vs_sequential": ens_rate / seq_rate,
+            "clocks": clk,
             "roofline": {"bound": "hbm", "bytes_per_cell_step": B_ENSEMBLE,
                          "achieved": ens_gbs, "peak": peak, "unit": "GB/s",
                          "frac": ens_gbs / peak, "peak_source": f"{peak_kind} hbm_gbs",
