@@ -65,7 +65,8 @@ B_STEP = B_DONOR + B_CORR_FACES + B_CORR_LAST  # 80 B per cell-step
 B_ENSEMBLE = 9 * 4
 B_ENSEMBLE_FUSED = 4 * 4
 FALLBACK_HBM_GBS = 6650.0
-# Arithmetic forms timed: "plain" = IEEE FP32 throughout; "precision_form" =
+# Arithmetic forms timed, all on the two-cell pass: "plain" = IEEE FP32
+# throughout (round-to-nearest division); "precision_form" =
 # FP32 storage and faces (hardware-reciprocal face ratios) with the limiter's
 # sums and ratios in FP64; "approx_div" = FP32 with hardware-reciprocal ratios
 # everywhere.  The headline value is the fastest form within the FP64 error
@@ -82,7 +83,7 @@ WORKLOAD_OPTS = {"vv_fix": True}
 ACC_STEPS = 100  # horizon of the FP64 accuracy check: the configuration's length
 # The corrective-pass kernel each form runs (the solver's default kernel choice).
 KERNEL_OF_FORM = {
-    "plain": "k_pass_tma<float, limiter> (fused corrective pass, one cell per thread)",
+    "plain": "k_pass_pair<limiter, IEEE division> (fused corrective pass, two cells per thread)",
     "precision_form": "k_pass_pair<limiter, approx, FP64 limiter ratios> (fused corrective pass, "
                       "two cells per thread)",
     "approx_div": "k_pass_pair<limiter, approx> (fused corrective pass, two cells per thread)",

@@ -341,6 +341,13 @@ int mpdata_step_noalloc(int nx, int ny, int ns, int order, int limiter, const fl
                         void* stream);
 
 /* Page-locked host memory for fast staging (cudaMallocHost / cudaFreeHost). */
+/* Self-check of the two-cell pass's division (no counterpart in the
+ * reference): n seeded random operand pairs of the ranges the pass divides,
+ * the division it uses without the library's slow path against IEEE
+ * round-to-nearest division; *mismatches = results that differ in any bit
+ * (0 expected).  Runs on the current device. */
+int mpdata_check_division(long long n, unsigned long long seed, long long* mismatches);
+
 void* mpdata_host_alloc(size_t bytes);
 void mpdata_host_free(void* p);
 

@@ -102,6 +102,17 @@ _lib.mpdata_pass_times.argtypes = [_vp, C.POINTER(C.c_double * 3), C.POINTER(C.c
                                    C.c_int]
 
 
+_lib.mpdata_check_division.argtypes = [C.c_longlong, C.c_ulonglong, C.POINTER(C.c_longlong)]
+
+
+def check_division(n: int, seed: int = 1) -> int:
+    """Bitwise mismatches between the two-cell pass's division and IEEE
+    division on n seeded random operand pairs (``mpdata_check_division``)."""
+    out = C.c_longlong(-1)
+    _check(_lib.mpdata_check_division(n, seed, C.byref(out)))
+    return out.value
+
+
 def last_error() -> str:
     return _lib.mpdata_last_error().decode()
 

@@ -89,10 +89,18 @@ __device__ __forceinline__ float2 pick(bool px, bool py, float2 a, float2 b)
 __device__ __forceinline__ float2 ld2(const float* p) { return *reinterpret_cast<const float2*>(p); }
 __device__ __forceinline__ void st2(float* p, float2 v) { *reinterpret_cast<float2*>(p) = v; }
 
+// Lane-wise n / d: hardware reciprocal (approx_div) or round-to-nearest
+// division without the slow-path call (div_nearest, IEEE results).
 template <bool AP> __device__ __forceinline__ float2 rat2(float2 n, float2 d)
 {
     if constexpr (AP) return n * make_float2(rcp_approx(d.x), rcp_approx(d.y));
-    else return make_float2(n.x / d.x, n.y / d.y);
+    else return make_float2(div_nearest(n.x, d.x), div_nearest(n.y, d.y));
+}
+// min(n / d, 1) lane-wise for n >= 0 (the limiter's clamped ratios).
+template <bool AP> __device__ __forceinline__ float2 rat2_min1(float2 n, float2 d)
+{
+    if constexpr (AP) return min2(rat2<true>(n, d), bc(1.f));
+    else return make_float2(div_nearest<true>(n.x, d.x), div_nearest<true>(n.y, d.y));
 }
 // Lane-wise sums with the pair's right neighbour: (a.x + a.y, a.y + b) and
 // differences (a.y - a.x, b - a.y).  Written as scalar operations: a paired
@@ -745,13 +753,15 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 // limited fluxes and of their sums then never lets a cell's
                 // limited out-fluxes exceed its margin above its lower bound, so a
                 // field with zeros stays non-negative.
-                float2 rup = rat2<AP>(mx - cq2, fin + eps), rdn = rat2<AP>(cq2 - mn, fout + eps);
                 if constexpr (WIDE) {
-                    rup = rup * bc(1.f - 0x1p-20f);
-                    rdn = rdn * bc(1.f - 0x1p-20f);
+                    const float2 rup = rat2<AP>(mx - cq2, fin + eps) * bc(1.f - 0x1p-20f);
+                    const float2 rdn = rat2<AP>(cq2 - mn, fout + eps) * bc(1.f - 0x1p-20f);
+                    bu = min2(rup, bc(1.f));
+                    bd = min2(rdn, bc(1.f));
+                } else {
+                    bu = rat2_min1<AP>(mx - cq2, fin + eps);
+                    bd = rat2_min1<AP>(cq2 - mn, fout + eps);
                 }
-                bu = min2(rup, bc(1.f));
-                bd = min2(rdn, bc(1.f));
                 if constexpr (WIDE) {
                     // A non-zero sum near zero (below 2^-100, where FLT_MIN and
                     // subnormal flux parts stop being negligible) is formed again in

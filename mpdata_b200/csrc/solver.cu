@@ -699,12 +699,14 @@ int mpd::create_solver(Solver** out, int nx, int ny, int ns, int dtype, int orde
     CUDA_TRY(cudaGetDevice(&h->device));
     CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
-    // The two-cell pass: FP32, fast arithmetic, fused kernels by default (with
-    // precision_form its limiter sums and ratios run in FP64).  With the limiter and
-    // IEEE division the one-cell pass is faster on B200 (the division slow paths
-    // spill the two-cell kernel's registers), so it keeps that form.
+    // The two-cell pass: FP32, fast arithmetic, fused kernels by default.  Its IEEE
+    // form divides by div_nearest (round-to-nearest results without the slow-path
+    // call that made the compiled division cost it registers); with precision_form
+    // it takes FP64 only for near-zero limiter sums, which needs approx_div -- the
+    // precision form with IEEE division (all limiter sums and ratios in FP64) stays
+    // on the one-cell pass.
     h->pair = o.kernel == 3 || (dtype == MPDATA_F32 && !o.strict && o.kernel == 0 &&
-                                (o.approx_div || !o.limiter));
+                                !(o.precision_form && !o.approx_div));
     h->zdepth = default_zdepth(h.get());
     if (int rc = alloc_solver(h.get())) {
         free_solver(h.get());

@@ -174,3 +174,14 @@ def test_pair_precision_form_near_zero_fields(m, approx):
         ref = oracle.step_faces(U, V, W, ref, 2, limiter=1, wide_beta=1)
     assert np.isfinite(got).all() and float(got.min()) >= 0.0
     assert float(np.abs(got - ref).max()) <= TOL
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_division_matches_ieee_bit_for_bit(m, seed):
+    """The IEEE form of the two-cell pass divides without the compiled
+    division's slow path (Newton-refined hardware reciprocal and Markstein's
+    remainder correction, IEEE division only for near-zero numerators): on
+    2^32 seeded operand pairs of the pass's ranges (divisors FLT_MIN..2^100,
+    numerators of either sign from zero and subnormals up), plain and clamped
+    to 1, every result equals IEEE round-to-nearest division bit for bit."""
+    assert m.check_division(1 << 32, seed) == 0
