@@ -547,7 +547,9 @@ def run_ensemble(m, torch, steps: int, base_steps: int):
     ens_gbs = ens_rate * B_ENSEMBLE  # Gcell-steps/s x bytes per cell-step = GB/s
     return {"value": ens_rate, "unit": UNIT, "instances": len(cfg), "steps": steps,
             "interior_cells_per_step": cells, "ms_per_step": t_ens / steps,
-            "tile": list(m.Ensemble.TILES[tile]), "autotune_ms_per_step": tune_ms,
+            "tile": list(m.Ensemble.TILES[tile]),
+            "kernel": "y-march (warp per 32-column strip)" if tile == m.Ensemble.MARCH
+                      else "tile kernel", "autotune_ms_per_step": tune_ms,
             "sequential": {"value": seq_rate, "steps": base_steps,
                            "ms_per_step": t_seq / base_steps,
                            "how": "256 per-instance solvers (nx x ny x 3), stepped one after another"},

@@ -289,7 +289,9 @@ int mpdata_ensemble_sync(mpdata_ensemble_handle e);
  * The trials advance the instances: set the fields again afterwards. */
 int mpdata_ensemble_autotune(mpdata_ensemble_handle e, int trial_steps, int* chosen,
                              double* ms_per_step);
-/* Force a tile-shape candidate (0: 32x8, 1: 32x16, 2: 64x8 threads). */
+/* Force a candidate: tile shapes 0: 32x8, 1: 32x16, 2: 64x8 threads; 3: the
+ * first corrective pass as a y-march (one warp per strip of 32 columns and 64
+ * rows, no shared memory or barriers), the other passes with shape 1. */
 int mpdata_ensemble_tile(mpdata_ensemble_handle e, int tile);
 
 /* ---- Adjoint of a window of steps ------------------------------------------

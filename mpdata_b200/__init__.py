@@ -433,7 +433,11 @@ class Ensemble:
     ``nx x ny x 3`` with w = 0), float32.  Faces and fields are 2D arrays of
     shape ``(ny, nx)``."""
 
-    TILES = ((32, 8), (32, 16), (64, 8))
+    # Candidates of the autotuner: tile shapes (threads x, y) of the tile
+    # kernels, and 3 = the y-march (the first corrective pass by one warp per
+    # strip of 32 columns x 64 rows, the other passes with tile 1).
+    TILES = ((32, 8), (32, 16), (64, 8), (32, 64))
+    MARCH = 3
 
     def __init__(self, nx, ny, order: int = 2, options: SolverOptions | None = None, **kw):
         opts = options or SolverOptions(**kw)

@@ -29,9 +29,14 @@ using mpd::Dims;
 
 namespace {
 
+// Tile shapes of the tile kernels.  Candidate kMarch runs the first
+// corrective pass as a y-march (one warp per strip of 32 columns x kMarchRows
+// rows, k_ens_march) and every other pass with tile kMarchTile.
 constexpr int kTiles = 3;
 const int kTileX[kTiles] = {32, 32, 64};
 const int kTileY[kTiles] = {8, 16, 8};
+constexpr int kMarch = kTiles, kMarchTile = 1, kCandidates = kTiles + 1;
+constexpr int kMarchRows = 64;
 
 struct GraphKey {
     int nsteps, cur;
@@ -50,7 +55,9 @@ struct mpdata_ensemble {
     // work lists per tile shape: [tile][0] donor items, [tile][1] pass items
     mpd::EnsItem* items[kTiles][2] = {{nullptr}};
     int nitems[kTiles][2] = {{0}};
-    int tile = 0;
+    mpd::EnsItem* march_items = nullptr;  // (instance, first owned column, rows [j0, pad))
+    int nmarch = 0;
+    int tile = 0;  // candidate 0 .. kCandidates-1
     int grid_donor = 0, grid_pass = 0;
     int cur = 0, prev = 0;
     int device = 0;
@@ -89,16 +96,37 @@ int build_items(mpdata_ensemble* e)
                                 cudaMemcpyHostToDevice));
             e->nitems[t][kind] = (int)v.size();
         }
+    // march strips: 26 owned columns of 32 lanes with the limiter (3 halo lanes
+    // each side), 28 without; chunks of kMarchRows owned rows
+    {
+        const int w = e->opts.limiter ? 26 : 28;
+        std::vector<mpd::EnsItem> v;
+        for (int q = 0; q < e->n; q++)
+            for (int j0 = 1; j0 <= e->ny[q] - 2; j0 += kMarchRows)
+                for (int i0 = 1; i0 <= e->nx[q] - 2; i0 += w)
+                    v.push_back({q, i0, j0, std::min(j0 + kMarchRows, e->ny[q] - 1)});
+        std::stable_sort(v.begin(), v.end(), [&](const mpd::EnsItem& a, const mpd::EnsItem& b) {
+            return (long long)e->nx[a.inst] * e->ny[a.inst] > (long long)e->nx[b.inst] * e->ny[b.inst];
+        });
+        CUDA_TRY(cudaMalloc(&e->march_items, std::max<size_t>(1, v.size()) * sizeof(mpd::EnsItem)));
+        CUDA_TRY(cudaMemcpy(e->march_items, v.data(), v.size() * sizeof(mpd::EnsItem),
+                            cudaMemcpyHostToDevice));
+        e->nmarch = (int)v.size();
+    }
     return 0;
 }
+
+// The tile kernels' shape for the current candidate.
+int tile_shape(const mpdata_ensemble* e) { return e->tile == kMarch ? kMarchTile : e->tile; }
 
 void set_grid(mpdata_ensemble* e)
 {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
     // persistent grids: a few CTAs per SM, never more than there are items
-    e->grid_donor = std::max(1, std::min(e->nitems[e->tile][0], sms * 8));
-    e->grid_pass = std::max(1, std::min(e->nitems[e->tile][1], sms * 4));
+    const int t = tile_shape(e);
+    e->grid_donor = std::max(1, std::min(e->nitems[t][0], sms * 8));
+    e->grid_pass = std::max(1, std::min(e->nitems[t][1], sms * 4));
 }
 
 template <bool STRICT>
@@ -111,14 +139,15 @@ void launch_step_passes(mpdata_ensemble* e, int& cur, int& prev)
     p.use_div = e->opts.div_mode != MPDATA_DIV_OFF;
     p.vv_fix = e->opts.vv_fix;
     p.fuse_donor = 0;
+    const int t = tile_shape(e);
     // With corrective passes, pass 1 forms c^(1) itself (level b1 is then not written)
     if (P == 1) {
         if (STRICT)
-            mpd::strict::launch_ens_donor<float>(e->tile, e->arena, e->insts, e->items[e->tile][0],
-                                                 e->nitems[e->tile][0], e->grid_donor, p, e->stream);
+            mpd::strict::launch_ens_donor<float>(t, e->arena, e->insts, e->items[t][0],
+                                                 e->nitems[t][0], e->grid_donor, p, e->stream);
         else
-            mpd::fast::launch_ens_donor<float>(e->tile, e->arena, e->insts, e->items[e->tile][0],
-                                               e->nitems[e->tile][0], e->grid_donor, p, e->stream);
+            mpd::fast::launch_ens_donor<float>(t, e->arena, e->insts, e->items[t][0],
+                                               e->nitems[t][0], e->grid_donor, p, e->stream);
     }
     int in = b1, out = b2;
     for (int o = 1; o < P; o++) {
@@ -128,14 +157,24 @@ void launch_step_passes(mpdata_ensemble* e, int& cur, int& prev)
         p.pass = o;
         p.write_faces = o < P - 1;
         p.fuse_donor = o == 1;
-        if (STRICT)
-            mpd::strict::launch_ens_pass<float>(e->tile, e->arena, e->insts, e->items[e->tile][1],
-                                                e->nitems[e->tile][1], e->grid_pass, p,
-                                                e->opts.limiter, e->opts.precision_form, 0, e->stream);
-        else
-            mpd::fast::launch_ens_pass<float>(e->tile, e->arena, e->insts, e->items[e->tile][1],
-                                              e->nitems[e->tile][1], e->grid_pass, p, e->opts.limiter,
-                                              e->opts.precision_form, e->opts.approx_div, e->stream);
+        // the march candidate runs the (fused) first pass as a y-march; the march
+        // has FP32 limiter ratios only, so the precision form keeps the tile kernel
+        if (o == 1 && e->tile == kMarch && !e->opts.precision_form) {
+            if (STRICT)
+                mpd::strict::launch_ens_march<float>(e->arena, e->insts, e->march_items, e->nmarch, p,
+                                                     e->opts.limiter, 0, e->stream);
+            else
+                mpd::fast::launch_ens_march<float>(e->arena, e->insts, e->march_items, e->nmarch, p,
+                                                   e->opts.limiter, e->opts.approx_div, e->stream);
+        } else if (STRICT) {
+            mpd::strict::launch_ens_pass<float>(t, e->arena, e->insts, e->items[t][1], e->nitems[t][1],
+                                                e->grid_pass, p, e->opts.limiter,
+                                                e->opts.precision_form, 0, e->stream);
+        } else {
+            mpd::fast::launch_ens_pass<float>(t, e->arena, e->insts, e->items[t][1], e->nitems[t][1],
+                                              e->grid_pass, p, e->opts.limiter, e->opts.precision_form,
+                                              e->opts.approx_div, e->stream);
+        }
         std::swap(in, out);
     }
     if (P == 1) { cur = b1; prev = b0; }
@@ -179,6 +218,7 @@ void destroy_ensemble(mpdata_ensemble* e)
     drop_graphs(e);
     for (int t = 0; t < kTiles; t++)
         for (int k = 0; k < 2; k++) cudaFree(e->items[t][k]);
+    cudaFree(e->march_items);
     cudaFree(e->insts);
     cudaFree(e->arena);
     if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
@@ -365,7 +405,7 @@ int mpdata_ensemble_autotune(mpdata_ensemble_handle e, int trial_steps, int* cho
     cudaEvent_t a, b;
     CUDA_TRY(cudaEventCreate(&a));
     CUDA_TRY(cudaEventCreate(&b));
-    for (int t = 0; t < kTiles; t++) {
+    for (int t = 0; t < kCandidates; t++) {
         e->tile = t;
         set_grid(e);
         run_steps_direct(e, 1);  // warm-up
@@ -393,7 +433,7 @@ int mpdata_ensemble_autotune(mpdata_ensemble_handle e, int trial_steps, int* cho
 
 int mpdata_ensemble_tile(mpdata_ensemble_handle e, int tile)
 {
-    if (!e || tile < 0 || tile >= kTiles) return mpd::fail(MPDATA_ERR_ARG, "bad tile %d", tile);
+    if (!e || tile < 0 || tile >= kCandidates) return mpd::fail(MPDATA_ERR_ARG, "bad tile %d", tile);
     e->tile = tile;
     set_grid(e);
     drop_graphs(e);

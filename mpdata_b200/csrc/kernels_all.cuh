@@ -46,6 +46,8 @@ template int launch_ens_pass<float>(int, float*, const EnsInst*, const EnsItem*,
                                     const EnsPass&, int, int, int, cudaStream_t);
 template int launch_ens_donor<float>(int, float*, const EnsInst*, const EnsItem*, int, int,
                                      const EnsPass&, cudaStream_t);
+template int launch_ens_march<float>(float*, const EnsInst*, const EnsItem*, int, const EnsPass&,
+                                     int, int, cudaStream_t);
 
 namespace {
 constexpr int kBX = 32, kBY = 8;

@@ -322,6 +322,168 @@ __global__ void __launch_bounds__(TX * TY)
     }
 }
 
+// ---- the first corrective pass as a y-march, one warp per item -------------
+//
+// An item is a strip of an instance: 32 consecutive columns (lane l holds
+// column x0 - LO + l) and a chunk of owned rows [ya, yb).  The warp marches
+// the rows upwards; every value a cell needs from a column to its left or
+// right comes from the neighbouring lane by a warp shuffle, every value of a
+// row below from registers carried by the march, so the pass uses no shared
+// memory and no barrier.  Iteration j: c^(1) of row j+1 (the donor update,
+// pass 0 fused as in k_ens_pass), the raw faces of row j (x face and the y
+// face above), with the limiter the ratios of row j and the limited faces
+// that need them, and the update of row j-1.  The arithmetic is k_ens_pass's
+// (the same face, limiter and donor functions on the same operands), so both
+// give the same bits.  Lanes whose columns lack a neighbour's operands only
+// feed their neighbours: owned lanes are LO .. 31 - HI (limiter: 3 .. 28).
+//
+// The items' i0 is the first owned column, j0 the first owned row, pad the
+// end of the owned rows.
+template <typename T, bool LIM, bool AP>
+__global__ void __launch_bounds__(128)
+    k_ens_march(T* __restrict__ arena, const EnsInst* __restrict__ insts,
+                const EnsItem* __restrict__ items, int nitems, EnsPass p)
+{
+    using namespace ens;
+    constexpr int LO = LIM ? 3 : 2, HI = LIM ? 3 : 2;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (it >= nitems) return;  // whole warps only: every lane of a warp takes this branch alike
+    const EnsItem item = items[it];
+    const EnsInst& in = insts[item.inst];
+    const int nx = in.nx, ny = in.ny, px = in.px;
+    const int i = item.i0 - LO + lane;  // this lane's column
+    const int ya = item.j0, yb = item.pad;
+    const T* gn = arena + in.c[p.cn];
+    const T* gu = arena + in.f[0][0];
+    const T* gv = arena + in.f[0][1];
+    T* gout = arena + in.c[p.out];
+    const bool col_ok = i >= 0 && i < px;
+    const bool own_lane = lane >= LO && lane <= 31 - HI;
+    auto ld = [&](const T* a, int row) -> T {
+        return (col_ok && row >= 0 && row < ny) ? a[(long long)row * px + i] : T(0);
+    };
+    auto left = [&](T v) { return __shfl_up_sync(FULL, v, 1); };
+    auto right = [&](T v) { return __shfl_down_sync(FULL, v, 1); };
+    auto left2 = [&](T v) { return __shfl_up_sync(FULL, v, 2); };
+    // c^(1) of row r from c^n rows r-1 (nm), r (nc), r+1 (np), the advective x
+    // face of row r (ur) and the y faces below (vm) and above (vc) the row:
+    // k_ens_pass's fused donor update for interior cells, the fixed shell
+    // copied, 0 outside the instance
+    auto c1_of = [&](int r, T nm, T nc, T np, T ur, T vm, T vc) -> T {
+        const T nl = left(nc), nr = right(nc), ul = left(ur);
+        if (i >= 1 && i <= nx - 2 && r >= 1 && r <= ny - 2) {
+            const T fx = upwind(nc, nr, ur) - upwind(nl, nc, ul);
+            const T fy = upwind(nc, np, vc) - upwind(nm, nc, vm);
+            return nc - T(0.5) * (fx + fy);
+        }
+        return nc;
+    };
+    // The march starts two rows below the first owned row: the ratios of row
+    // ya-1 need the raw y face below it.  Registers by row relative to j.
+    const int j_first = ya - 2;
+    T nm1 = ld(gn, j_first - 1), n0 = ld(gn, j_first), np1 = ld(gn, j_first + 1);
+    T np2 = ld(gn, j_first + 2);
+    T u0 = ld(gu, j_first), up1 = ld(gu, j_first + 1);
+    T vm1 = ld(gv, j_first - 1), v0 = ld(gv, j_first), vp1 = ld(gv, j_first + 1);
+    T cm2, cm1, c0;  // c^(1) of rows j-2, j-1, j
+    {
+        const T n_m3 = ld(gn, j_first - 3), n_m2 = ld(gn, j_first - 2);
+        const T v_m3 = ld(gv, j_first - 3), v_m2 = ld(gv, j_first - 2);
+        cm2 = c1_of(j_first - 2, n_m3, n_m2, nm1, ld(gu, j_first - 2), v_m3, v_m2);
+        cm1 = c1_of(j_first - 1, n_m2, nm1, n0, ld(gu, j_first - 1), v_m2, vm1);
+        c0 = c1_of(j_first, nm1, n0, np1, u0, vm1, v0);
+    }
+    // Carried faces: the raw y face below row j (rv_prev), the x face of row
+    // j-1 and the y face (j-2|j-1) in the form the update uses (limited with
+    // the limiter), the ratios of row j-1.
+    T rv_prev = T(0), fx_prev = T(0), fy_pp = T(0);
+    T bu_prev = T(1), bd_prev = T(1);
+    for (int j = j_first; j <= yb; j++) {
+        // operands of the next iteration (latency overlaps this one)
+        const T n_next = ld(gn, j + 3), u_next = ld(gu, j + 2), v_next = ld(gv, j + 2);
+        const T cp1 = c1_of(j + 1, n0, np1, np2, up1, v0, vp1);
+        // ---- raw faces of row j ----
+        Nb2<T> nb;
+        nb.C = c0; nb.L = left(c0); nb.R = right(c0); nb.D = cm1; nb.Uu = cp1;
+        nb.RU = right(cp1); nb.RD = right(cm1); nb.LU = left(cp1);
+        nb.u = u0; nb.uL = left(u0); nb.uR = right(u0); nb.uL2 = left2(u0);
+        nb.uLU = left(up1); nb.uU = up1; nb.uL2U = left2(up1);
+        nb.v = v0; nb.vD = vm1; nb.vU = vp1; nb.vR = right(v0); nb.vRD = right(vm1);
+        T ru = T(0), rv = T(0);
+        if (i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2) ru = face_u2<AP, true>(nb, i, nx, p.use_div);
+        if (i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2)
+            rv = face_v2<AP, true>(nb, i, j, ny, p.use_div, p.vv_fix, p.pass, v0);
+        const T ru_l = left(ru);
+        // ---- the faces the update of row j-1 uses ----
+        T fx_cur, fy_cur;  // x face of row j, y face (j-1|j)
+        T bu = T(1), bd = T(1);
+        if (LIM) {
+            const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
+            const T psi = c0, cl = nb.L, cr = nb.R, cd = cm1, cu = cp1;
+            const T nl = left(n0), nr = right(n0);
+            if (cell_in) {
+                T mx = vmax(psi, n0), mn = vmin(psi, n0);
+                mx = vmax(vmax(cl, nl), mx); mn = vmin(vmin(cl, nl), mn);
+                mx = vmax(vmax(cr, nr), mx); mn = vmin(vmin(cr, nr), mn);
+                mx = vmax(vmax(cd, nm1), mx); mn = vmin(vmin(cd, nm1), mn);
+                mx = vmax(vmax(cu, np1), mx); mn = vmin(vmin(cu, np1), mn);
+                T fin = T(0), fout = T(0);
+                lim_acc(lim_flux<T, T>(ru_l, cl, psi), false, fin, fout);
+                lim_acc(lim_flux<T, T>(ru, psi, cr), true, fin, fout);
+                lim_acc(lim_flux<T, T>(rv_prev, cd, psi), false, fin, fout);
+                lim_acc(lim_flux<T, T>(rv, psi, cu), true, fin, fout);
+                bu = ratio<AP>(mx - psi, fin + lim_tiny<T>());
+                bd = ratio<AP>(psi - mn, fout + lim_tiny<T>());
+            }
+            fx_cur = limit_face(ru, bu, bd, right(bu), right(bd));
+            fy_cur = limit_face(rv_prev, bu_prev, bd_prev, bu, bd);
+        } else {
+            fx_cur = ru;
+            fy_cur = rv_prev;
+        }
+        // ---- update of row r = j-1 ----
+        const int r = j - 1;
+        {
+            const T ul = left(fx_prev);
+            const T fxx = upwind(cm1, right(cm1), fx_prev) - upwind(left(cm1), cm1, ul);
+            const T fyy = upwind(cm1, c0, fy_cur) - upwind(cm2, cm1, fy_pp);
+            const T out = cm1 - T(0.5) * (fxx + fyy);
+            const bool owned = own_lane && r >= ya && r < yb && i >= 1 && i <= nx - 2 &&
+                               r >= 1 && r <= ny - 2;
+            if (owned) {
+                const long long q = (long long)r * px + i;
+                gout[q] = out;
+                if (p.write_faces) {
+                    arena[in.f[p.ws][0] + q] = fx_prev;
+                    arena[in.f[p.ws][1] + q] = fy_cur;
+                    if (i == 1) arena[in.f[p.ws][0] + q - 1] = ul;
+                    if (r == 1) arena[in.f[p.ws][1] + q - px] = fy_pp;
+                }
+            }
+        }
+        // ---- rotate ----
+        fy_pp = fy_cur;
+        fx_prev = fx_cur;
+        rv_prev = rv;
+        bu_prev = bu;
+        bd_prev = bd;
+        cm2 = cm1; cm1 = c0; c0 = cp1;
+        nm1 = n0; n0 = np1; np1 = np2; np2 = n_next;
+        u0 = up1; up1 = u_next;
+        vm1 = v0; v0 = vp1; vp1 = v_next;
+    }
+}
+
+template <typename T, bool LIM, bool AP>
+void ens_launch_march(T* arena, const EnsInst* insts, const EnsItem* items, int nitems,
+                      const EnsPass& p, cudaStream_t s)
+{
+    const int grid = (nitems + 3) / 4;
+    if (grid > 0) k_ens_march<T, LIM, AP><<<grid, 128, 0, s>>>(arena, insts, items, nitems, p);
+}
+
 template <typename T, bool LIM, typename A, bool AP, int TX, int TY>
 void ens_launch_pass(T* arena, const EnsInst* insts, const EnsItem* items, int nitems, int grid,
                      const EnsPass& p, cudaStream_t s)
@@ -367,6 +529,21 @@ int launch_ens_pass(int tile, T* arena, const EnsInst* insts, const EnsItem* ite
     case 1: ens_pass_tile<T, 32, 16>(arena, insts, items, nitems, grid, p, limiter, wide, approx, s); break;
     case 2: ens_pass_tile<T, 64, 8>(arena, insts, items, nitems, grid, p, limiter, wide, approx, s); break;
     default: return -1;
+    }
+    return 0;
+}
+
+// The first corrective pass as a y-march (k_ens_march; FP32 limiter ratios only).
+template <typename T>
+int launch_ens_march(T* arena, const EnsInst* insts, const EnsItem* items, int nitems,
+                     const EnsPass& p, int limiter, int approx, cudaStream_t s)
+{
+    if (limiter) {
+        if (approx) ens_launch_march<T, true, true>(arena, insts, items, nitems, p, s);
+        else ens_launch_march<T, true, false>(arena, insts, items, nitems, p, s);
+    } else {
+        if (approx) ens_launch_march<T, false, true>(arena, insts, items, nitems, p, s);
+        else ens_launch_march<T, false, false>(arena, insts, items, nitems, p, s);
     }
     return 0;
 }

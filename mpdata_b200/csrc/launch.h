@@ -113,6 +113,9 @@ template <typename T> struct AdjPassArgs {
                         int nitems, int grid, const EnsPass& p, int limiter, int wide,     \
                         int approx, cudaStream_t s);                                       \
     template <typename T>                                                                  \
+    int launch_ens_march(T* arena, const EnsInst* insts, const EnsItem* items, int nitems, \
+                         const EnsPass& p, int limiter, int approx, cudaStream_t s);       \
+    template <typename T>                                                                  \
     int launch_ens_donor(int tile, T* arena, const EnsInst* insts, const EnsItem* items,   \
                          int nitems, int grid, const EnsPass& p, cudaStream_t s);          \
     /* Faces of planes [k0, k0 + nk). */                                                   \

@@ -41,7 +41,7 @@ def _three_plane(m, inst, steps, order, **opts):
         return s.get_field()[1]
 
 
-@pytest.mark.parametrize("tile", [0, 1, 2])
+@pytest.mark.parametrize("tile", [0, 1, 2, 3])
 @pytest.mark.parametrize("limiter", [0, 1])
 @pytest.mark.parametrize("order", [1, 2, 3])
 @pytest.mark.parametrize("graph", [True, False], ids=["graph", "direct"])
@@ -87,7 +87,7 @@ def test_ensemble_autotune_picks_a_candidate_and_keeps_results():
             e.set_faces(q, d["U"].astype(np.float32), d["V"].astype(np.float32))
             e.set_field(q, d["c0"].astype(np.float32))
         tile, ms = e.autotune(trial_steps=3)
-        assert tile in (0, 1, 2) and ms > 0
+        assert tile in (0, 1, 2, 3) and ms > 0
         for q, d in enumerate(cfg):  # the trials advanced the fields: set them again
             e.set_field(q, d["c0"].astype(np.float32))
         e.step(5)
@@ -100,8 +100,9 @@ def test_ensemble_autotune_picks_a_candidate_and_keeps_results():
     assert got.min() >= 0.0
 
 
+@pytest.mark.parametrize("tile", [1, 3], ids=["tile", "march"])
 @pytest.mark.parametrize("strict", [True, False], ids=["strict", "default"])
-def test_ensemble_matches_cpu_oracle_sample(strict):
+def test_ensemble_matches_cpu_oracle_sample(strict, tile):
     """A sample of the benchmark-kind instances (rotation, Gaussian blob,
     IORD 2 + limiter) against the CPU oracle on the 3-plane form directly:
     strict arithmetic bit-identical, default within max-abs 1e-5."""
@@ -113,6 +114,7 @@ def test_ensemble_matches_cpu_oracle_sample(strict):
     steps = 6
     with m.Ensemble([d["nx"] for d in cfg], [d["ny"] for d in cfg], order=2, limiter=True,
                     strict=strict) as e:
+        e.set_tile(tile)
         for q, d in enumerate(cfg):
             e.set_faces(q, f32(d["U"]), f32(d["V"]))
             e.set_field(q, f32(d["c0"]))
