@@ -36,7 +36,10 @@ constexpr int kTiles = 3;
 const int kTileX[kTiles] = {32, 32, 64};
 const int kTileY[kTiles] = {8, 16, 8};
 constexpr int kMarch = kTiles, kMarchTile = 1, kCandidates = kTiles + 1;
-constexpr int kMarchRows = 64;
+#ifndef MPD_MARCH_ROWS
+#define MPD_MARCH_ROWS 64
+#endif
+constexpr int kMarchRows = MPD_MARCH_ROWS;
 
 struct GraphKey {
     int nsteps, cur;
