@@ -367,13 +367,14 @@ __global__ void __launch_bounds__(128)
     auto left = [&](T v) { return __shfl_up_sync(FULL, v, 1); };
     auto right = [&](T v) { return __shfl_down_sync(FULL, v, 1); };
     auto left2 = [&](T v) { return __shfl_up_sync(FULL, v, 2); };
-    // c^(1) of row r from c^n rows r-1 (nm), r (nc), r+1 (np), the advective x
-    // face of row r (ur) and the y faces below (vm) and above (vc) the row:
-    // k_ens_pass's fused donor update for interior cells, the fixed shell
-    // copied, 0 outside the instance
-    auto c1_of = [&](int r, T nm, T nc, T np, T ur, T vm, T vc) -> T {
-        const T nl = left(nc), nr = right(nc), ul = left(ur);
-        if (i >= 1 && i <= nx - 2 && r >= 1 && r <= ny - 2) {
+    // c^(1) of row r from c^n rows r-1 (nm), r (nc, its left / right
+    // neighbours nl, nr), r+1 (np), the advective x faces of row r (ur, and
+    // ul of the column to the left) and the y faces below (vm) and above (vc)
+    // the row: k_ens_pass's fused donor update for interior cells, the fixed
+    // shell copied, 0 outside the instance
+    auto c1_of = [&](bool border, int r, T nm, T nc, T np, T nl, T nr, T ur, T ul, T vm,
+                     T vc) -> T {
+        if (!border || (i >= 1 && i <= nx - 2 && r >= 1 && r <= ny - 2)) {
             const T fx = upwind(nc, nr, ur) - upwind(nl, nc, ul);
             const T fy = upwind(nc, np, vc) - upwind(nm, nc, vm);
             return nc - T(0.5) * (fx + fy);
@@ -381,7 +382,9 @@ __global__ void __launch_bounds__(128)
         return nc;
     };
     // The march starts two rows below the first owned row: the ratios of row
-    // ya-1 need the raw y face below it.  Registers by row relative to j.
+    // ya-1 need the raw y face below it.  Registers by row relative to j; the
+    // neighbours' values a later iteration needs again are carried (suffix
+    // L / R / L2: the lane to the left / right / two to the left).
     const int j_first = ya - 2;
     T nm1 = ld(gn, j_first - 1), n0 = ld(gn, j_first), np1 = ld(gn, j_first + 1);
     T np2 = ld(gn, j_first + 2);
@@ -391,42 +394,57 @@ __global__ void __launch_bounds__(128)
     {
         const T n_m3 = ld(gn, j_first - 3), n_m2 = ld(gn, j_first - 2);
         const T v_m3 = ld(gv, j_first - 3), v_m2 = ld(gv, j_first - 2);
-        cm2 = c1_of(j_first - 2, n_m3, n_m2, nm1, ld(gu, j_first - 2), v_m3, v_m2);
-        cm1 = c1_of(j_first - 1, n_m2, nm1, n0, ld(gu, j_first - 1), v_m2, vm1);
-        c0 = c1_of(j_first, nm1, n0, np1, u0, vm1, v0);
+        const T u_m2 = ld(gu, j_first - 2), u_m1 = ld(gu, j_first - 1);
+        cm2 = c1_of(true, j_first - 2, n_m3, n_m2, nm1, left(n_m2), right(n_m2), u_m2, left(u_m2),
+                    v_m3, v_m2);
+        cm1 = c1_of(true, j_first - 1, n_m2, nm1, n0, left(nm1), right(nm1), u_m1, left(u_m1),
+                    v_m2, vm1);
+        c0 = c1_of(true, j_first, nm1, n0, np1, left(n0), right(n0), u0, left(u0), vm1, v0);
     }
+    T cL0 = left(c0), cR0 = right(c0), cLm1 = left(cm1), cRm1 = right(cm1);
+    T nL0 = left(n0), nR0 = right(n0);
+    T uL0 = left(u0), uR0 = right(u0), uL20 = left2(u0);
+    T vR0 = right(v0), vRm1 = right(vm1);
     // Carried faces: the raw y face below row j (rv_prev), the x face of row
     // j-1 and the y face (j-2|j-1) in the form the update uses (limited with
     // the limiter), the ratios of row j-1.
     T rv_prev = T(0), fx_prev = T(0), fy_pp = T(0);
     T bu_prev = T(1), bd_prev = T(1);
-    for (int j = j_first; j <= yb; j++) {
+    // Strips whose every column takes the interior forms run rows 1 .. ny-3
+    // through a copy without the boundary cases (uniform over the warp).
+    const bool strip_in = item.i0 - LO >= 2 && item.i0 - LO + 31 <= nx - 3;
+
+    auto iteration = [&](auto border_tag, const int j) {
+        constexpr bool BORDER = decltype(border_tag)::value;
         // operands of the next iteration (latency overlaps this one)
         const T n_next = ld(gn, j + 3), u_next = ld(gu, j + 2), v_next = ld(gv, j + 2);
-        const T cp1 = c1_of(j + 1, n0, np1, np2, up1, v0, vp1);
+        const T npL = left(np1), npR = right(np1);
+        const T upL = left(up1), upR = right(up1), upL2 = left2(up1);
+        const T vpR = right(vp1);
+        const T cp1 = c1_of(BORDER, j + 1, n0, np1, np2, npL, npR, up1, upL, v0, vp1);
+        const T cpL = left(cp1), cpR = right(cp1);
         // ---- raw faces of row j ----
         Nb2<T> nb;
-        nb.C = c0; nb.L = left(c0); nb.R = right(c0); nb.D = cm1; nb.Uu = cp1;
-        nb.RU = right(cp1); nb.RD = right(cm1); nb.LU = left(cp1);
-        nb.u = u0; nb.uL = left(u0); nb.uR = right(u0); nb.uL2 = left2(u0);
-        nb.uLU = left(up1); nb.uU = up1; nb.uL2U = left2(up1);
-        nb.v = v0; nb.vD = vm1; nb.vU = vp1; nb.vR = right(v0); nb.vRD = right(vm1);
+        nb.C = c0; nb.L = cL0; nb.R = cR0; nb.D = cm1; nb.Uu = cp1;
+        nb.RU = cpR; nb.RD = cRm1; nb.LU = cpL;
+        nb.u = u0; nb.uL = uL0; nb.uR = uR0; nb.uL2 = uL20;
+        nb.uLU = upL; nb.uU = up1; nb.uL2U = upL2;
+        nb.v = v0; nb.vD = vm1; nb.vU = vp1; nb.vR = vR0; nb.vRD = vRm1;
         T ru = T(0), rv = T(0);
-        if (i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2) ru = face_u2<AP, true>(nb, i, nx, p.use_div);
-        if (i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2)
-            rv = face_v2<AP, true>(nb, i, j, ny, p.use_div, p.vv_fix, p.pass, v0);
+        if (!BORDER || (i >= 0 && i <= nx - 2 && j >= 1 && j <= ny - 2))
+            ru = face_u2<AP, BORDER>(nb, i, nx, p.use_div);
+        if (!BORDER || (i >= 1 && i <= nx - 2 && j >= 0 && j <= ny - 2))
+            rv = face_v2<AP, BORDER>(nb, i, j, ny, p.use_div, p.vv_fix, p.pass, v0);
         const T ru_l = left(ru);
         // ---- the faces the update of row j-1 uses ----
         T fx_cur, fy_cur;  // x face of row j, y face (j-1|j)
         T bu = T(1), bd = T(1);
         if (LIM) {
-            const bool cell_in = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2;
-            const T psi = c0, cl = nb.L, cr = nb.R, cd = cm1, cu = cp1;
-            const T nl = left(n0), nr = right(n0);
-            if (cell_in) {
+            const T psi = c0, cl = cL0, cr = cR0, cd = cm1, cu = cp1;
+            if (!BORDER || (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2)) {
                 T mx = vmax(psi, n0), mn = vmin(psi, n0);
-                mx = vmax(vmax(cl, nl), mx); mn = vmin(vmin(cl, nl), mn);
-                mx = vmax(vmax(cr, nr), mx); mn = vmin(vmin(cr, nr), mn);
+                mx = vmax(vmax(cl, nL0), mx); mn = vmin(vmin(cl, nL0), mn);
+                mx = vmax(vmax(cr, nR0), mx); mn = vmin(vmin(cr, nR0), mn);
                 mx = vmax(vmax(cd, nm1), mx); mn = vmin(vmin(cd, nm1), mn);
                 mx = vmax(vmax(cu, np1), mx); mn = vmin(vmin(cu, np1), mn);
                 T fin = T(0), fout = T(0);
@@ -447,7 +465,7 @@ __global__ void __launch_bounds__(128)
         const int r = j - 1;
         {
             const T ul = left(fx_prev);
-            const T fxx = upwind(cm1, right(cm1), fx_prev) - upwind(left(cm1), cm1, ul);
+            const T fxx = upwind(cm1, cRm1, fx_prev) - upwind(cLm1, cm1, ul);
             const T fyy = upwind(cm1, c0, fy_cur) - upwind(cm2, cm1, fy_pp);
             const T out = cm1 - T(0.5) * (fxx + fyy);
             const bool owned = own_lane && r >= ya && r < yb && i >= 1 && i <= nx - 2 &&
@@ -470,9 +488,17 @@ __global__ void __launch_bounds__(128)
         bu_prev = bu;
         bd_prev = bd;
         cm2 = cm1; cm1 = c0; c0 = cp1;
+        cLm1 = cL0; cRm1 = cR0; cL0 = cpL; cR0 = cpR;
         nm1 = n0; n0 = np1; np1 = np2; np2 = n_next;
+        nL0 = npL; nR0 = npR;
         u0 = up1; up1 = u_next;
+        uL0 = upL; uR0 = upR; uL20 = upL2;
         vm1 = v0; v0 = vp1; vp1 = v_next;
+        vRm1 = vR0; vR0 = vpR;
+    };
+    for (int j = j_first; j <= yb; j++) {
+        if (strip_in && j >= 1 && j <= ny - 3) iteration(std::false_type{}, j);
+        else iteration(std::true_type{}, j);
     }
 }
 
