@@ -37,7 +37,7 @@ const int kTileX[kTiles] = {32, 32, 64};
 const int kTileY[kTiles] = {8, 16, 8};
 constexpr int kMarch = kTiles, kMarchTile = 1, kCandidates = kTiles + 1;
 #ifndef MPD_MARCH_ROWS
-#define MPD_MARCH_ROWS 64
+#define MPD_MARCH_ROWS 48
 #endif
 constexpr int kMarchRows = MPD_MARCH_ROWS;
 
