@@ -57,7 +57,7 @@ constexpr int WX = 36, WY = CY + 1, WPL = WX * WY;  // work planes: x [-2, 33], 
 __host__ __device__ constexpr int stage_bytes() { return (SBX * SBY * 4 + 127) / 128 * 128; }
 // staged arrays: c, Uo, Vo, Wo (+ c^n with the limiter)
 template <bool LIM> __host__ __device__ constexpr int n_arrays() { return LIM ? 5 : 4; }
-template <bool LIM> __host__ __device__ constexpr int n_work() { return LIM ? 12 : 2; }
+template <bool LIM> __host__ __device__ constexpr int n_work() { return LIM ? 10 : 2; }
 template <bool LIM> __host__ __device__ constexpr size_t smem_bytes()
 {
     return (size_t)NSTAGE * n_arrays<LIM>() * stage_bytes() + (size_t)n_work<LIM>() * WPL * 4 +
@@ -79,6 +79,19 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __
 __device__ __forceinline__ float2 abs2(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
 __device__ __forceinline__ float2 max2(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
 __device__ __forceinline__ float2 min2(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
+// Three-input max / min (PTX max.f32 / min.f32 with three operands, sm_100).
+__device__ __forceinline__ float max3f(float a, float b, float c)
+{
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c)
+{
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
 // (a.y, b) and (a, b.x): the pair shifted by one cell to the right / left.
 __device__ __forceinline__ float2 sh(float2 a, float b) { return make_float2(a.y, b); }
 __device__ __forceinline__ float2 shl(float a, float2 b) { return make_float2(a, b.x); }
@@ -522,9 +535,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
     float* work = reinterpret_cast<float*>(smem + (size_t)NSTAGE * NARR * SB);
     float* sFX = work;           // limiter fluxes through the raw x faces of plane k (A|B, B|x+2)
     float* sFY = sFX + WPL;      // through the raw y faces
-    float* sMX = sFY + WPL;      // bound extrema max / min(c, c^n) of plane k
-    float* sMN = sMX + WPL;
-    float* sBU = sMN + WPL;      // ratios (clamped to <= 1), two slots by plane parity
+    float* sBU = sFY + WPL;      // ratios (clamped to <= 1), two slots by plane parity
     float* sBD = sBU + 2 * WPL;
     float* sDX = sBD + 2 * WPL;  // donor fluxes through the limited faces, two slots
     float* sDY = sDX + 2 * WPL;
@@ -666,8 +677,8 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
         if (!HA) return;
         // ---- raw faces of plane k (z: face k+1/2), limiter fluxes, bound extrema ----
         const bool kin = k >= 1 && k <= ns - 2;
-        float2 ru, rv, rw, cU, fyH, fzH, mx0, mn0;
-        float c2, fxI, fxH;
+        float2 ru, rv, rw, cU, cD, fyH, fzH;
+        float c2, cL, fxI, fxH;
         {
             if (k + 1 <= ns - 1) {
                 if (ok) ok = tma::mbar_wait(&bars[SP1], ((k + 1 - kstart) / NSTAGE) & 1);
@@ -687,22 +698,19 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 }
                 rw = face_z<AP, BORDER>(nb, qs, p.g, k == 0, k == ns - 2, a.use_div);
                 c2 = nb.c_2;
+                cL = nb.c_m1;
                 cU = nb.cU;
+                cD = nb.cD;
             } else {  // the top shell plane: no faces
-                ru = rv = rw = cU = bc(0.f);
-                c2 = 0.f;
+                ru = rv = rw = cU = cD = bc(0.f);
+                c2 = cL = 0.f;
             }
             fxI = flux(ru.x, cq2.x, cq2.y);
             fxH = flux(ru.y, cq2.y, c2);
             fyH = flux2(rv, cq2, cU);
             fzH = flux2(rw, cq2, cq3);
-            const float2 cn0 = ld2(slot(S, 4) + p.o);
-            mx0 = max2(cq2, cn0);
-            mn0 = min2(cq2, cn0);
             st2(sFX + p.w, make_float2(fxI, fxH));
             st2(sFY + p.w, fyH);
-            st2(sMX + p.w, mx0);
-            st2(sMN + p.w, mn0);
         }
         __syncthreads();
 
@@ -723,27 +731,25 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
                 const float2 py = max2(fyL, z0v), pz = max2(fzL, z0v);
                 const float2 hy = max2(fyH, z0v), hz = max2(fzH, z0v);
 
-                // bounds over the cell and its face neighbours (z only in 3D)
+                // bounds over the cell and its face neighbours (z only in 3D): max /
+                // min of c and c^n over the seven cells, every value from the staged
+                // planes or registers (the pair's own two cells are shared by both
+                // lanes), with three-input min / max
                 const float* cnS = slot(S, 4);
-                const float mAB = fmaxf(mx0.x, mx0.y), nAB = fminf(mn0.x, mn0.y);
-                // edge threads: the neighbour's extrema from the staged planes;
-                // both forms evaluated and selected (no divergent branch)
-                const float cnR = cnS[p.o + 2];
-                const float2 cnU = ld2(cnS + p.o + Y);
-                const float mRs = sMX[p.w + 2], nRs = sMN[p.w + 2];
-                const float2 mUs = ld2(sMX + p.w + WX), nUs = ld2(sMN + p.w + WX);
-                const float mR = edge_x ? fmaxf(c2, cnR) : mRs;
-                const float nR = edge_x ? fminf(c2, cnR) : nRs;
-                const float2 mU = edge_y ? max2(cU, cnU) : mUs;
-                const float2 nU = edge_y ? min2(cU, cnU) : nUs;
-                float2 mx = make_float2(fmaxf(mAB, sMX[p.w - 1]), fmaxf(mAB, mR));
-                float2 mn = make_float2(fminf(nAB, sMN[p.w - 1]), fminf(nAB, nR));
-                mx = max2(mx, max2(ld2(sMX + p.w - WX), mU));
-                mn = min2(mn, min2(ld2(sMN + p.w - WX), nU));
+                const float2 cn0 = ld2(cnS + p.o), cnD = ld2(cnS + p.o - Y), cnU = ld2(cnS + p.o + Y);
+                const float cnL = cnS[p.o - 1], cnR = cnS[p.o + 2];
+                const float mAB = max3f(cq2.x, cq2.y, fmaxf(cn0.x, cn0.y));
+                const float nAB = min3f(cq2.x, cq2.y, fminf(cn0.x, cn0.y));
+                float2 mx = make_float2(max3f(max3f(mAB, cL, cnL), max3f(cD.x, cnD.x, cU.x), cnU.x),
+                                        max3f(max3f(mAB, c2, cnR), max3f(cD.y, cnD.y, cU.y), cnU.y));
+                float2 mn = make_float2(min3f(min3f(nAB, cL, cnL), min3f(cD.x, cnD.x, cU.x), cnU.x),
+                                        min3f(min3f(nAB, c2, cnR), min3f(cD.y, cnD.y, cU.y), cnU.y));
                 if (ns > 3) {
                     const float2 cnm = ld2(slot(SM1, 4) + p.o), cnp = ld2(slot(SP1, 4) + p.o);
-                    mx = max2(mx, max2(max2(cq1, cnm), max2(cq3, cnp)));
-                    mn = min2(mn, min2(min2(cq1, cnm), min2(cq3, cnp)));
+                    mx = make_float2(max3f(mx.x, max3f(cq1.x, cnm.x, cq3.x), cnp.x),
+                                     max3f(mx.y, max3f(cq1.y, cnm.y, cq3.y), cnp.y));
+                    mn = make_float2(min3f(mn.x, min3f(cq1.x, cnm.x, cq3.x), cnp.x),
+                                     min3f(mn.y, min3f(cq1.y, cnm.y, cq3.y), cnp.y));
                 }
                 const float2 fin = finx + ((py + pz) + ((hy - fyH) + (hz - fzH)));
                 const float2 fout = foutx + (((py - fyL) + (pz - fzL)) + (hy + hz));
