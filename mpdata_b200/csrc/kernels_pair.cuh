@@ -327,11 +327,14 @@ __device__ __forceinline__ float2 face_z(const PairNb& n, const PairSums& q, con
     return r;
 }
 
-// Limited face: a min(1, beta_out(lo), beta_in(hi)) for a > 0, a min(1, beta_in(lo),
-// beta_out(hi)) otherwise; the ratios are stored already clamped to <= 1.
-__device__ __forceinline__ float limit(float a, float bu_lo, float bd_lo, float bu_hi, float bd_hi)
+// Limiter factor of a face: min(1, beta_out(lo), beta_in(hi)) for a > 0,
+// min(1, beta_in(lo), beta_out(hi)) otherwise; the ratios are stored already
+// clamped to <= 1.  The limited face is a times it, and its flux (upwind
+// value from the same c) the raw face's flux times it.
+__device__ __forceinline__ float lim_factor(float a, float bu_lo, float bd_lo, float bu_hi,
+                                            float bd_hi)
 {
-    return a * (a > 0.f ? fminf(bd_lo, bu_hi) : fminf(bu_lo, bd_hi));
+    return a > 0.f ? fminf(bd_lo, bu_hi) : fminf(bu_lo, bd_hi);
 }
 
 }  // namespace pair
@@ -599,6 +602,8 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
     float2 cq2 = ok ? ld2(slot(kstart & (NSTAGE - 1), 0) + p.o) : bc(0.f), cq3 = bc(0.f);
     float2 ru_prev = bc(0.f), rv_prev = bc(0.f);  // raw x / y faces of plane k-1
     float2 rw_prev = bc(0.f), rw_pp = bc(0.f);    // raw z faces k-1/2 and k-3/2
+    float2 fx_prev = bc(0.f), fy_prev = bc(0.f);  // their limiter fluxes (x: A|B, B|x+2)
+    float2 fz_prev = bc(0.f), fz_pp = bc(0.f);
     float2 dz_prev = bc(0.f);                     // donor flux through the limited z face k-5/2
     long long qk = p.col + (long long)kstart * pp;  // element offset of the pair in plane k
 
@@ -622,34 +627,30 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
             const float* bd1 = sBD + PM * WPL;
             const float2 bu = ld2(bu1 + p.w), bd = ld2(bd1 + p.w);
             const float2 bu2 = ld2(sBU + PK * WPL + p.w), bd2 = ld2(sBD + PK * WPL + p.w);
-            float2 lu = ru_prev, lv = rv_prev;
-            lu.x = limit(ru_prev.x, bu.x, bd.x, bu.y, bd.y);
-            // The edge threads' outer faces (x = 31|32, y = CY-1|CY) have no ratio on
-            // the far side in this CTA and stay raw (no kept cell uses them); both
+            // Limiter factors; the donor fluxes through the limited faces are the
+            // raw faces' fluxes (formed with the same c) times them.  The edge
+            // threads' outer faces (x = 31|32, y = CY-1|CY) have no ratio on the far
+            // side in this CTA and stay raw (factor 1; no kept cell uses them); both
             // forms are evaluated and selected, without a divergent branch (the far
             // reads stay inside shared memory: x + 2 <= 33 < WX, and row CY + 1 of
             // a ratio plane is the first row of the next work array).
-            {
-                const float buR = bu1[p.w + 2], bdR = bd1[p.w + 2];
-                const float2 buU = ld2(bu1 + p.w + WX), bdU = ld2(bd1 + p.w + WX);
-                const float luy = limit(ru_prev.y, bu.y, bd.y, buR, bdR);
-                const float2 lvl = make_float2(limit(rv_prev.x, bu.x, bd.x, buU.x, bdU.x),
-                                               limit(rv_prev.y, bu.y, bd.y, buU.y, bdU.y));
-                lu.y = edge_x ? ru_prev.y : luy;
-                lv = edge_y ? rv_prev : lvl;
-            }
-            const float2 lw = make_float2(limit(rw_pp.x, bu2.x, bd2.x, bu.x, bd.x),
-                                          limit(rw_pp.y, bu2.y, bd2.y, bu.y, bd.y));
-            const float* cm = slot(SM1, 0);  // staged c of plane k-1
-            const float c2m = cm[p.o + 2];
-            const float2 cUm = ld2(cm + p.o + Y);
-            const float2 dx = make_float2(flux(lu.x, cq1.x, cq1.y), flux(lu.y, cq1.y, c2m));
-            const float2 dy = flux2(lv, cq1, cUm);
-            const float2 dz = flux2(lw, cq0, cq1);  // face k-3/2
+            const float buR = bu1[p.w + 2], bdR = bd1[p.w + 2];
+            const float2 buU = ld2(bu1 + p.w + WX), bdU = ld2(bd1 + p.w + WX);
+            const float myB = lim_factor(ru_prev.y, bu.y, bd.y, buR, bdR);
+            const float2 gx = make_float2(lim_factor(ru_prev.x, bu.x, bd.x, bu.y, bd.y),
+                                          edge_x ? 1.f : myB);
+            float2 gy = make_float2(lim_factor(rv_prev.x, bu.x, bd.x, buU.x, bdU.x),
+                                    lim_factor(rv_prev.y, bu.y, bd.y, buU.y, bdU.y));
+            if (edge_y) gy = bc(1.f);
+            const float2 gz = make_float2(lim_factor(rw_pp.x, bu2.x, bd2.x, bu.x, bd.x),
+                                          lim_factor(rw_pp.y, bu2.y, bd2.y, bu.y, bd.y));
+            const float2 dx = gx * fx_prev, dy = gy * fy_prev;
+            const float2 dz = gz * fz_pp;  // face k-3/2
             st2(sDX + PM * WPL + p.w, dx);
             st2(sDY + PM * WPL + p.w, dy);
             const long long q1 = qk - pp;  // plane k-1
             if (a.write_faces) {
+                const float2 lu = gx * ru_prev, lv = gy * rv_prev, lw = gz * rw_pp;
                 if (k - 1 >= z0 && k - 1 < z1) {
                     if (p.wxA) a.Un[q1] = lu.x;
                     if (p.wxB) a.Un[q1 + 1] = lu.y;
@@ -720,7 +721,7 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
             if (kin) {
                 const float fxL = sFX[p.w - 1];
                 const float2 fyL = ld2(sFY + p.w - WX);
-                const float2 fzL = flux2(rw_prev, cq1, cq2);  // raw z face k-1/2
+                const float2 fzL = fz_prev;  // raw z face k-1/2
                 // in: positive low-face and negative high-face fluxes; out: the rest
                 // (max(f,0) - f = max(-f,0)).  x lane-wise: A's faces are L|A and
                 // A|B, B's are A|B and B|x+2.
@@ -815,6 +816,10 @@ __device__ __forceinline__ void pair_march_lim(const Dims& d, const PassArgs<flo
         rv_prev = rv;
         rw_pp = rw_prev;
         rw_prev = rw;
+        fx_prev = make_float2(fxI, fxH);
+        fy_prev = fyH;
+        fz_pp = fz_prev;
+        fz_prev = fzH;
         qk += pp;
     };
     for (int kb = kstart & ~(NSTAGE - 1); kb <= last; kb += NSTAGE) {
