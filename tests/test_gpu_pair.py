@@ -76,12 +76,22 @@ def test_pair_pass_agrees_with_one_cell_pass(m, shape, opt):
     assert float(np.abs(a - b).max()) <= TOL
 
 
+FORMS = {"ieee": dict(), "approx": dict(approx=True),
+         "precision": dict(approx=True, precision_form=True)}
+
+
 @pytest.mark.parametrize("depth", [1, 2, 3, 7, 0])
 @pytest.mark.parametrize("limiter", [0, 1])
-def test_pair_pass_z_chunks_bit_identical(m, depth, limiter):
+@pytest.mark.parametrize("form", list(FORMS))
+def test_pair_pass_z_chunks_bit_identical(m, depth, limiter, form):
+    """A march split into z chunks of any depth equals the whole-column
+    march bit for bit, for the unrolled (approx_div) and the rolled (IEEE,
+    precision) plane loops."""
+    if form == "precision" and not limiter:
+        pytest.skip("the precision form acts on the limiter")
     shape = (70, 40, 26)
-    full, _ = _run(m, shape, 3, dict(limiter=limiter), 2, depth=0, seed=9)
-    got, _ = _run(m, shape, 3, dict(limiter=limiter), 2, depth=depth, seed=9)
+    full, _ = _run(m, shape, 3, dict(limiter=limiter), 2, depth=0, seed=9, **FORMS[form])
+    got, _ = _run(m, shape, 3, dict(limiter=limiter), 2, depth=depth, seed=9, **FORMS[form])
     assert np.array_equal(full, got)
 
 
