@@ -20,9 +20,12 @@
 //    equal the reference's formulas up to rounding (not bit for bit), so
 //    strict mode keeps k_pass_tma.
 //  * Neighbours exchange fluxes, not raw values: the limiter's in/out
-//    fluxes of each cell's high faces, the cells' bound extrema, the ratios
-//    (clamped to <= 1) and the donor fluxes F = a (a > 0 ? c_lo : c_hi),
-//    so the donor update needs no neighbour c values.
+//    fluxes of each cell's high faces, the ratios (clamped to <= 1) and the
+//    donor fluxes F = a (a > 0 ? c_lo : c_hi), so the donor update needs no
+//    neighbour c values.  A donor flux is the raw face's limiter flux,
+//    carried from the plane before, times the limiter factor.
+//  * The limiter's bounds come from the staged planes and the values the
+//    faces read, with three-input min / max.
 //  * No extra low faces are formed: the CTA's cells overlap their
 //    neighbours' (with the limiter x 0..2 and 31, rows 0, 1 and CY-1 are not
 //    updated; without it x 0 and 31 and row 0), so every face a kept cell
