@@ -59,11 +59,14 @@ struct mpdata_adjoint {
     std::vector<std::array<void*, 3>> lam_L;
     void* lam_R[3] = {nullptr, nullptr, nullptr};
     void* lam_B[2] = {nullptr, nullptr};
-    // The accumulators every adjoint step starts from zero (lam_lev[1..P-1],
-    // lam_L, then lam_R and lam_B) share one allocation, cleared by one memset
-    // per step; lam_R + lam_B are contiguous at its end.
+    // The accumulators every adjoint step starts from zero share one
+    // allocation, cleared by one memset per step: lam_L of the passes before
+    // the last (later passes scatter into them) and, at its end, lam_B (the
+    // ratio adjoints, scattered into by every pass and cleared again before
+    // each earlier pass).  lam_lev[1..P-1], lam_L of the last pass and lam_R
+    // are written (=) by each pass's first kernel and need no clearing.
     void* zblock = nullptr;
-    size_t zblock_bytes = 0, zRB_bytes = 0;
+    size_t zblock_bytes = 0, zB_bytes = 0;
     bool have_faces = false;
     // A full segment of the backward sweep (replay + adjoint steps) as a CUDA
     // graph, captured on first use; one per parity of the adjoint buffers at
@@ -158,6 +161,7 @@ int step_adj(mpdata_adjoint* h, mpdata_adjoint::Record& R, const T* lam_next, T*
     for (int o = P - 1; o >= 0; o--) {
         mpd::AdjPassArgs<T> a{};
         a.pass = o;
+        a.accum_F = o < P - 1;
         a.limiter = h->opts.limiter;
         a.wide = h->opts.precision_form;
         a.use_div = h->opts.div_mode != MPDATA_DIV_OFF;
@@ -177,7 +181,7 @@ int step_adj(mpdata_adjoint* h, mpdata_adjoint::Record& R, const T* lam_next, T*
             a.bup = (const T*)R.B[o][0]; a.bdn = (const T*)R.B[o][1];
             if (h->opts.limiter) {
                 // cleared with the block for the step's last pass; again for earlier passes
-                if (o != P - 1) CUDA_TRY(cudaMemsetAsync(h->lam_R[0], 0, h->zRB_bytes, h->stream));
+                if (o != P - 1) CUDA_TRY(cudaMemsetAsync(h->lam_B[0], 0, h->zB_bytes, h->stream));
                 a.lRU = (T*)h->lam_R[0]; a.lRV = (T*)h->lam_R[1]; a.lRW = (T*)h->lam_R[2];
                 a.lbup = (T*)h->lam_B[0]; a.lbdn = (T*)h->lam_B[1];
             }
@@ -359,7 +363,12 @@ int mpdata_adjoint_create(mpdata_adjoint_handle* out, int nx, int ny, int ns, in
     H->lam_lev.resize(order + 2);
     H->lam_L.resize(order);
     const size_t fb = field_bytes(H);
-    const int nz = 4 * (order - 1) + (H->opts.limiter ? 5 : 0);
+    for (int o = 1; o < order && !rc; o++) rc = A(&H->lam_lev[o]);
+    if (order > 1)
+        for (int a = 0; a < 3 && !rc; a++) rc = A(&H->lam_L[order - 1][a]);
+    if (H->opts.limiter)
+        for (int a = 0; a < 3 && !rc; a++) rc = A(&H->lam_R[a]);
+    const int nz = 3 * std::max(order - 2, 0) + (H->opts.limiter ? 2 : 0);
     if (!rc && nz > 0) {
         if (cudaMalloc(&H->zblock, nz * fb) != cudaSuccess) {
             rc = mpd::fail(MPDATA_ERR_CUDA, "adjoint allocation failed");
@@ -367,12 +376,10 @@ int mpdata_adjoint_create(mpdata_adjoint_handle* out, int nx, int ny, int ns, in
             H->blocks.push_back(H->zblock);
             H->zblock_bytes = nz * fb;
             char* z = (char*)H->zblock;
-            for (int o = 1; o < order; o++) { H->lam_lev[o] = z; z += fb; }
-            for (int o = 1; o < order; o++)
+            for (int o = 1; o < order - 1; o++)
                 for (int a = 0; a < 3; a++) { H->lam_L[o][a] = z; z += fb; }
             if (H->opts.limiter) {
-                H->zRB_bytes = 5 * fb;
-                for (int a = 0; a < 3; a++) { H->lam_R[a] = z; z += fb; }
+                H->zB_bytes = 2 * fb;
                 for (int a = 0; a < 2; a++) { H->lam_B[a] = z; z += fb; }
             }
         }

@@ -73,17 +73,56 @@ __device__ __forceinline__ PatAdj<T> pattern_adj(T lam, T a, T lo, T hi, T b1, T
     return g;
 }
 
+// Limiter application adjoint of one face (forward: k_fct_apply, L = R g,
+// g = the frozen min of 1 and the two ratios): lR = g l, and a l to the
+// ratio the min selected.  q / hq: the face's low / high cell, lo_in / hi_in:
+// whether they are interior (shell cells have no ratio: 1).
+template <typename T>
+__device__ __forceinline__ void limit_face_adj(T a, T l, long long q, long long hq, bool lo_in,
+                                               bool hi_in, const T* bup, const T* bdn, T* lR,
+                                               T* lbup, T* lbdn)
+{
+    const T bu_lo = lo_in ? bup[q] : T(1), bd_lo = lo_in ? bdn[q] : T(1);
+    const T bu_hi = hi_in ? bup[hq] : T(1), bd_hi = hi_in ? bdn[hq] : T(1);
+    T x, y;
+    T *lx, *ly;  // adjoint slots of the two candidate ratios (null for the shell)
+    if (a > T(0)) { x = bd_lo; y = bu_hi; lx = lo_in ? lbdn : nullptr; ly = hi_in ? lbup : nullptr; }
+    else { x = bu_lo; y = bd_hi; lx = lo_in ? lbup : nullptr; ly = hi_in ? lbdn : nullptr; }
+    const bool pick_x = x < y;
+    const T g1 = pick_x ? x : y;
+    const bool ratio_sel = g1 < T(1);
+    const T g = ratio_sel ? g1 : T(1);
+    lR[q] = g * l;  // the first contribution of the step (the ratio adjoint adds later)
+    if (ratio_sel) {
+        if (pick_x) acc(lx, q, a * l);
+        else acc(ly, hq, a * l);
+    }
+}
+
+// Arrays of the limiter-application adjoint, fused into the donor adjoint of
+// a corrective pass (all null without the limiter and for pass 0).
+template <typename T> struct LimAdj {
+    const T *RU, *RV, *RW, *bup, *bdn;
+    T *lRU, *lRV, *lRW, *lbup, *lbdn;
+};
+
 }  // namespace adj
 
 // Donor pass adjoint (forward: k_donor).  One thread per cell of the full grid:
 // gathers the cell's adjoint (identity for every cell, shell included, plus
 // the flux terms of its six faces) and, when lamF is given, the adjoint of
-// its three high faces.  lam_in and lamF accumulate (+=).
+// its three high faces.  lam_in accumulates (+=) when add_in is set and is
+// written (=) otherwise (the first kernel of the step to touch it); lamF
+// adds to what earlier kernels accumulated there when add_F is set.  With
+// the limiter (lim.lRU set) the adjoint of each high face goes on at once
+// through the limiter application (the faces the donor update read are
+// L = R g) to the raw face and the ratios, in place of a kernel of its own,
+// and lamF is not written; without it lamF is written (=).
 template <typename T>
 __global__ void k_adj_donor(Dims d, const T* __restrict__ c, const T* __restrict__ U,
                             const T* __restrict__ V, const T* __restrict__ W,
                             const T* __restrict__ lam_out, T* __restrict__ lam_in, T* lamU, T* lamV,
-                            T* lamW)
+                            T* lamW, adj::LimAdj<T> lim, int add_in, int add_F)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -116,7 +155,18 @@ __global__ void k_adj_donor(Dims d, const T* __restrict__ c, const T* __restrict
             const T sg = A > T(0) ? T(1) : T(-1);
             const T dF = T(0.5) * ((inner(a, 1) ? lam_out[q + S[a]] : T(0)) - lq);
             lam += dF * (A * (T(1) + sg));
-            if (lF[a]) lF[a][q] += dF * (c[q] * (T(1) + sg) + c[q + S[a]] * (T(1) - sg));
+            if (lF[a]) {
+                const T lf = dF * (c[q] * (T(1) + sg) + c[q + S[a]] * (T(1) - sg));
+                const T l = add_F ? lF[a][q] + lf : lf;
+                if (lim.lRU) {
+                    const T* R[3] = {lim.RU, lim.RV, lim.RW};
+                    T* lR[3] = {lim.lRU, lim.lRV, lim.lRW};
+                    adj::limit_face_adj(R[a][q], l, q, q + S[a], me_in, inner(a, 1), lim.bup,
+                                        lim.bdn, lR[a], lim.lbup, lim.lbdn);
+                } else {
+                    lF[a][q] = l;
+                }
+            }
         }
         if (face_used(a, idx[a] - 1)) {  // low face: this cell is hi
             const T A = F[a][q - S[a]];
@@ -125,49 +175,7 @@ __global__ void k_adj_donor(Dims d, const T* __restrict__ c, const T* __restrict
             lam += dF * (A * (T(1) - sg));
         }
     }
-    lam_in[q] += lam;
-}
-
-// Limiter application adjoint (forward: k_fct_apply, L = R * g, g = the
-// frozen min of 1 and the two ratios).
-template <typename T>
-__global__ void k_adj_limit(Dims d, const T* __restrict__ RU, const T* __restrict__ RV,
-                            const T* __restrict__ RW, const T* __restrict__ bup,
-                            const T* __restrict__ bdn, const T* __restrict__ lLU,
-                            const T* __restrict__ lLV, const T* __restrict__ lLW, T* lRU, T* lRV,
-                            T* lRW, T* lbup, T* lbdn)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = blockIdx.z;
-    if (i >= d.nx || j >= d.ny) return;
-    const long long q = cell(d, i, j, k);
-    const int nx = d.nx, ny = d.ny, ns = d.ns;
-    const bool kin = k >= 1 && k <= ns - 2, jin = j >= 1 && j <= ny - 2, iin = i >= 1 && i <= nx - 2;
-    auto one = [&](const T* R, const T* lL, T* lR, long long hq, int hi, int hj, int hk) {
-        const T a = R[q];
-        const bool lo_in = adj::interior(d, i, j, k), hi_in = adj::interior(d, hi, hj, hk);
-        const T bu_lo = lo_in ? bup[q] : T(1), bd_lo = lo_in ? bdn[q] : T(1);
-        const T bu_hi = hi_in ? bup[hq] : T(1), bd_hi = hi_in ? bdn[hq] : T(1);
-        T x, y;
-        T *lx, *ly;  // adjoint slots of the two candidate ratios (null for the shell)
-        long long qx = q, qy = hq;
-        if (a > T(0)) { x = bd_lo; y = bu_hi; lx = lo_in ? lbdn : nullptr; ly = hi_in ? lbup : nullptr; }
-        else { x = bu_lo; y = bd_hi; lx = lo_in ? lbup : nullptr; ly = hi_in ? lbdn : nullptr; }
-        const bool pick_x = x < y;
-        const T g1 = pick_x ? x : y;
-        const bool ratio_sel = g1 < T(1);
-        const T g = ratio_sel ? g1 : T(1);
-        const T l = lL[q];
-        lR[q] += g * l;
-        if (ratio_sel) {
-            if (pick_x) adj::acc(lx, qx, a * l);
-            else adj::acc(ly, qy, a * l);
-        }
-    };
-    if (kin && jin && i <= nx - 2) one(RU, lLU, lRU, q + 1, i + 1, j, k);
-    if (kin && iin && j <= ny - 2) one(RV, lLV, lRV, q + d.px, i, j + 1, k);
-    if (jin && iin && k <= ns - 2) one(RW, lLW, lRW, q + d.pp, i, j, k + 1);
+    lam_in[q] = add_in ? lam_in[q] + lam : lam;
 }
 
 // Limiter ratio adjoint (forward: k_fct_beta), one thread per interior cell.
@@ -391,13 +399,16 @@ template <typename T>
 void launch_adj_pass(const Dims& d, const AdjPassArgs<T>& a, cudaStream_t s)
 {
     dim3 b(32, 8), g((d.nx + 31) / 32, (d.ny + 7) / 8, d.ns);
-    // donor part of this pass (faces F = limited faces, or advective for pass 0)
-    k_adj_donor<T><<<g, b, 0, s>>>(d, a.c, a.FU, a.FV, a.FW, a.lam_out, a.lam_in, a.lFU, a.lFV, a.lFW);
+    // donor part of this pass (faces F = limited faces, or advective for pass 0),
+    // with the limiter application's adjoint fused in
+    adj::LimAdj<T> lim{};
+    if (a.pass > 0 && a.limiter)
+        lim = adj::LimAdj<T>{a.RU, a.RV, a.RW, a.bup, a.bdn, a.lRU, a.lRV, a.lRW, a.lbup, a.lbdn};
+    k_adj_donor<T><<<g, b, 0, s>>>(d, a.c, a.FU, a.FV, a.FW, a.lam_out, a.lam_in, a.lFU, a.lFV, a.lFW,
+                                   lim, a.pass == 0, a.accum_F);
     if (a.pass == 0) return;
     const T* lRU = a.lFU; const T* lRV = a.lFV; const T* lRW = a.lFW;
     if (a.limiter) {
-        k_adj_limit<T><<<g, b, 0, s>>>(d, a.RU, a.RV, a.RW, a.bup, a.bdn, a.lFU, a.lFV, a.lFW, a.lRU,
-                                       a.lRV, a.lRW, a.lbup, a.lbdn);
         if (a.wide)
             k_adj_beta<T, double><<<g, b, 0, s>>>(d, a.c, a.cn, a.RU, a.RV, a.RW, a.lbup, a.lbdn,
                                                   a.lam_in, a.lam_cn, a.lRU, a.lRV, a.lRW);

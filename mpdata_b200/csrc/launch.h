@@ -86,16 +86,17 @@ struct EnsPass {
 // Adjoint of one pass o of a step (kernels_adjoint.cuh).
 template <typename T> struct AdjPassArgs {
     int pass, limiter, wide, use_div, vv_fix;
+    int accum_F;                   // lFU.. hold a later pass's contributions (o < P-1)
     const T *c, *cn;               // level c_o, step input c_0
     const T *FU, *FV, *FW;         // faces of this pass's donor update (advective for o = 0)
     const T *RU, *RV, *RW;         // raw antidiffusive faces of pass o
     const T *bup, *bdn;            // limiter ratios of pass o
     const T *Uo, *Vo, *Wo;         // previous faces (the pattern's inputs)
     const T* lam_out;              // adjoint of c_{o+1}
-    T* lam_in;                     // adjoint of c_o (+=)
+    T* lam_in;                     // adjoint of c_o (written by the donor part; += for o = 0)
     T* lam_cn;                     // adjoint of c_0 (+=, limiter bounds)
-    T *lFU, *lFV, *lFW;            // adjoint of this pass's donor faces (+=; null for o = 0)
-    T *lRU, *lRV, *lRW;            // adjoint of the raw faces (+=; limiter only)
+    T *lFU, *lFV, *lFW;            // adjoint of this pass's donor faces (null for o = 0)
+    T *lRU, *lRV, *lRW;            // adjoint of the raw faces (limiter only)
     T *lbup, *lbdn;                // adjoint of the ratios (+=)
     T *lUo, *lVo, *lWo;            // adjoint of the previous faces (+=; null if advective)
 };
