@@ -43,24 +43,28 @@ template <typename T>
 __device__ __forceinline__ PatAdj<T> pattern_adj(T lam, T a, T lo, T hi, T b1, T n1, T d1, T b2,
                                                  T n2, T d2, bool has_div, T sdiv)
 {
+    // Three reciprocals (of d1, d2 and the first term's denominator) stand
+    // for the dozen quotients of the derivative.
     PatAdj<T> g;
-    const T r1 = (b1 * n1) / d1, r2 = (b2 * n2) / d2;
+    const T id1 = T(1) / d1, id2 = T(1) / d2;
+    const T r1 = (b1 * n1) * id1, r2 = (b2 * n2) * id2;
     const T sg = a > T(0) ? T(1) : T(-1);
     const T m = a > T(0) ? a : -a;
     const T num = (m * (T(1) - m)) * (hi - lo);
-    const T den = (hi + lo) + tiny<T>();
+    const T iden = T(1) / ((hi + lo) + tiny<T>());
     // out = t - 0.5 a (r1 + r2)
     const T lr = T(-0.5) * a * lam;
+    const T lr1 = lr * id1, lr2 = lr * id2;
     g.a = T(-0.5) * (r1 + r2) * lam;
-    g.b1 = lr * n1 / d1;
-    g.n1 = lr * b1 / d1;
-    g.d1 = -lr * r1 / d1;
-    g.b2 = lr * n2 / d2;
-    g.n2 = lr * b2 / d2;
-    g.d2 = -lr * r2 / d2;
+    g.b1 = lr1 * n1;
+    g.n1 = lr1 * b1;
+    g.d1 = -lr1 * r1;
+    g.b2 = lr2 * n2;
+    g.n2 = lr2 * b2;
+    g.d2 = -lr2 * r2;
     // t = neg_div + num / den
-    const T lnum = lam / den;
-    const T lden = -lam * (num / den) / den;
+    const T lnum = lam * iden;
+    const T lden = -lnum * (num * iden);
     const T lm = lnum * (T(1) - T(2) * m) * (hi - lo);
     g.hi = lnum * (m * (T(1) - m)) + lden;
     g.lo = -lnum * (m * (T(1) - m)) + lden;
