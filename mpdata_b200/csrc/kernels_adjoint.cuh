@@ -227,11 +227,12 @@ __global__ void k_adj_beta(Dims d, const T* __restrict__ c, const T* __restrict_
         fl[f] = lim_flux<T, A>(a, c[lo[f]], c[hi[f]]);
         lim_acc(fl[f], (f & 1) != 0, fin, fout);
     }
-    const A din = fin + lim_tiny<A>(), dout = fout + lim_tiny<A>();
-    const A bu = (A(mx) - A(psi)) / din, bd = (A(psi) - A(mn)) / dout;
-    const A l_mx = A(lu) / din, l_mn = -A(ld) / dout;
-    const A l_psi = -A(lu) / din + A(ld) / dout;
-    const A l_fin = -A(lu) * bu / din, l_fout = -A(ld) * bd / dout;
+    // two reciprocals for the eight quotients of the derivative
+    const A idin = A(1) / (fin + lim_tiny<A>()), idout = A(1) / (fout + lim_tiny<A>());
+    const A bu = (A(mx) - A(psi)) * idin, bd = (A(psi) - A(mn)) * idout;
+    const A l_mx = A(lu) * idin, l_mn = -A(ld) * idout;
+    const A l_psi = -l_mx - l_mn;
+    const A l_fin = -l_mx * bu, l_fout = l_mn * bd;
     adj::acc(arr[imx] == c ? lam_c : lam_cn, q + off[imx], T(l_mx));
     adj::acc(arr[imn] == c ? lam_c : lam_cn, q + off[imn], T(l_mn));
     adj::acc(lam_c, q, T(l_psi));
