@@ -130,8 +130,13 @@ class ClockSampler:
         self.path = None
 
     def start(self):
+        """Start sampling and return once the sampler has written its first
+        row (nvidia-smi needs ~0.1-0.5 s to start), so the timed region that
+        follows is covered from its beginning; rows written before that are
+        dropped by stop()."""
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
+        self.skip = 0
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
@@ -139,6 +144,15 @@ class ClockSampler:
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        t_end = time.time() + 5.0
+        while time.time() < t_end and self.proc.poll() is None:
+            with open(self.path) as f:
+                n = sum(1 for line in f if line.endswith("\n"))
+            if n:
+                self.skip = n
+                break
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
@@ -149,7 +163,11 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         rows = []
-        for line in open(self.path):
+        lines = open(self.path).readlines()
+        # rows written before the timed region; keep them only if nothing came after
+        if len(lines) > self.skip:
+            lines = lines[self.skip:]
+        for line in lines:
             p = [x.strip() for x in line.split(",")]
             if len(p) < 9:
                 continue
