@@ -3,6 +3,8 @@
 Checks (tolerances stated here):
   * FP64 adjoint vs central finite differences of the FP64 forward window
     along random directions: relative error <= 1e-6;
+  * the dot-product identity <M v, w> = <v, M^T w> of the linear (order 1)
+    step: relative 1e-12 (FP64);
   * FP32 adjoint vs the FP64 adjoint: relative L2 <= 1e-4;
   * the checkpoint interval does not change the gradient (FP64, 1e-10);
   * the torch.autograd.Function harness: a receptor loss differentiated with
@@ -65,6 +67,21 @@ def test_adjoint_matches_finite_differences_fp64(order, limiter):
         fd = (fp - fm) / (2 * eps)
         ad = float(np.sum(g * v))
         assert abs(fd - ad) <= 1e-6 * max(abs(fd), 1e-3), (fd, ad)
+
+
+@pytest.mark.parametrize("nsteps", [1, 4])
+def test_dot_product_identity_of_the_linear_step_fp64(nsteps):
+    """Order 1 (the donor-cell pass alone) is linear in c, c^N = M c^0, so the
+    adjoint must be its exact transpose: <M v, w> = <v, M^T w> to FP64
+    rounding (relative 1e-12), for dense random v and w of both signs."""
+    faces, c0, rng = _setup(seed=31 + nsteps)
+    v = rng.standard_normal(c0.shape)
+    w = rng.standard_normal(c0.shape)
+    mv = _fwd(faces, v, nsteps, 1)
+    mtw = _grad(faces, v, w, nsteps, 1)  # the transpose does not depend on the state
+    lhs, rhs = float(np.sum(mv * w)), float(np.sum(v * mtw))
+    scale = float(np.sum(np.abs(mv * w)))
+    assert abs(lhs - rhs) <= 1e-12 * scale, (lhs, rhs)
 
 
 @pytest.mark.parametrize("limiter", [0, 1])
