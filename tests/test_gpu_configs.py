@@ -14,6 +14,8 @@
   the FP64 oracle bit for bit after 128 steps; the FP32 forms (plain, the
   precision form, approx_div) stay within relative L2 1e-5 of it with no
   negative cell; zero-flux mass drift <= 1e-6 (FP32) and 1e-12 (FP64).
+  The same checks with the y faces of the x = 1 column computed (vv_fix)
+  against the FP64 oracle under that rule.
 * the throughput grid (512 x 512 x 256), plain IORD 3 without the limiter (the
   reference has none), 2 steps through smolar(): strict arithmetic
   bit-identical to the reference's own smolar(); default arithmetic within
@@ -170,6 +172,37 @@ def test_ring3d_fp64_strict_equals_oracle(m, ring3d_case, ring3d_fp64):
 def test_ring3d_fp32_forms_against_fp64(m, ring3d_case, ring3d_fp64, form):
     got, m0, m1, mn, nneg = _solver_run(m, ring3d_case, np.float32, STEPS3, **form)
     rel = float(np.linalg.norm(got - ring3d_fp64) / np.linalg.norm(ring3d_fp64))
+    assert rel <= 1e-5, rel
+    assert nneg == 0 and mn >= 0.0
+    assert abs(m1 - m0) / m0 <= 1e-6, abs(m1 - m0) / m0
+
+
+# The same configuration with the y faces of the x = 1 column computed
+# (vv_fix) instead of the reference's buffer rule for the column vv_pass
+# leaves unwritten: the FP64 oracle and the GPU under that rule.
+
+@pytest.fixture(scope="module")
+def ring3d_fp64_fix(ring3d_case, oracle_mod):
+    U, V, W, c = ring3d_case
+    for _ in range(STEPS3):
+        c = oracle_mod.step_faces(U, V, W, c, 2, limiter=1, vv_fix=1)
+    return c
+
+
+def test_ring3d_column_rule_fp64_strict_equals_oracle(m, ring3d_case, ring3d_fp64_fix):
+    got, m0, m1, mn, nneg = _solver_run(m, ring3d_case, np.float64, STEPS3, strict=True,
+                                        vv_fix=True)
+    assert np.array_equal(got, ring3d_fp64_fix)
+    assert nneg == 0 and mn >= 0.0
+    assert abs(m1 - m0) / m0 <= 1e-12
+
+
+@pytest.mark.parametrize("form", [dict(), dict(precision_form=True, approx_div=True),
+                                  dict(approx_div=True)],
+                         ids=["plain", "precision_form", "approx_div"])
+def test_ring3d_column_rule_fp32_forms_against_fp64(m, ring3d_case, ring3d_fp64_fix, form):
+    got, m0, m1, mn, nneg = _solver_run(m, ring3d_case, np.float32, STEPS3, vv_fix=True, **form)
+    rel = float(np.linalg.norm(got - ring3d_fp64_fix) / np.linalg.norm(ring3d_fp64_fix))
     assert rel <= 1e-5, rel
     assert nneg == 0 and mn >= 0.0
     assert abs(m1 - m0) / m0 <= 1e-6, abs(m1 - m0) / m0

@@ -100,12 +100,14 @@ def test_ensemble_autotune_picks_a_candidate_and_keeps_results():
     assert got.min() >= 0.0
 
 
+@pytest.mark.parametrize("vv_fix", [False, True], ids=["ref_column", "vv_fix"])
 @pytest.mark.parametrize("tile", [1, 3], ids=["tile", "march"])
 @pytest.mark.parametrize("strict", [True, False], ids=["strict", "default"])
-def test_ensemble_matches_cpu_oracle_sample(strict, tile):
+def test_ensemble_matches_cpu_oracle_sample(strict, tile, vv_fix):
     """A sample of the benchmark-kind instances (rotation, Gaussian blob,
     IORD 2 + limiter) against the CPU oracle on the 3-plane form directly:
-    strict arithmetic bit-identical, default within max-abs 1e-5."""
+    strict arithmetic bit-identical, default within max-abs 1e-5; under both
+    rules for the y faces of the x = 1 column."""
     import oracle
 
     import mpdata_b200 as m
@@ -113,7 +115,7 @@ def test_ensemble_matches_cpu_oracle_sample(strict, tile):
     f32 = lambda a: np.ascontiguousarray(a, np.float32)
     steps = 6
     with m.Ensemble([d["nx"] for d in cfg], [d["ny"] for d in cfg], order=2, limiter=True,
-                    strict=strict) as e:
+                    strict=strict, vv_fix=vv_fix) as e:
         e.set_tile(tile)
         for q, d in enumerate(cfg):
             e.set_faces(q, f32(d["U"]), f32(d["V"]))
@@ -126,7 +128,7 @@ def test_ensemble_matches_cpu_oracle_sample(strict, tile):
         U[1] = f32(d["U"]); V[1] = f32(d["V"])
         c = np.repeat(f32(d["c0"])[None], 3, 0)
         for _ in range(steps):
-            c = oracle.step_faces(U, V, np.zeros_like(U), c, 2, limiter=1)
+            c = oracle.step_faces(U, V, np.zeros_like(U), c, 2, limiter=1, vv_fix=int(vv_fix))
         if strict:
             assert np.array_equal(g, c[1]), q
         else:
