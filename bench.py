@@ -90,6 +90,24 @@ KERNEL_OF_FORM = {
 }
 
 
+# Solver kernel choices (mpdata_options.kernel) that --kernel can force on the
+# timed forms, for profiling captures of the other kernels; forms a kernel
+# cannot run (approx_div needs the fused kernels) are dropped.
+KERNEL_CHOICES = {
+    1: "k_antidiff + k_fct_beta + k_fct_apply + k_donor (one kernel per reference routine)",
+    2: "k_pass_tma<limiter> (fused corrective pass, one cell per thread)",
+    3: None,  # the two-cell pass: the default labels above
+}
+
+
+def _set_kernel(kernel):
+    global FORMS, KERNEL_OF_FORM
+    forms = [(n, o) for n, o in FORMS if not (kernel == 1 and o.get("approx_div"))]
+    FORMS = [(n, dict(o, kernel=kernel)) for n, o in forms]
+    if KERNEL_CHOICES[kernel] is not None:
+        KERNEL_OF_FORM = {n: KERNEL_CHOICES[kernel] for n, _ in FORMS}
+
+
 def config_text():
     return (f"roofline: {NX}x{NY}x{NS} FP32, IORD {ORDER} + nonoscillatory limiter, "
             "streamfunction flow, y faces of the x = 1 column computed (vv_fix)")
@@ -994,9 +1012,14 @@ def main():
                     help="print the FP64 error breakdown of the FP32 forms (no timing)")
     ap.add_argument("--size", default=None,
                     help="nx,ny,ns override (profiling captures of a smaller grid only)")
+    ap.add_argument("--kernel", type=int, default=None, choices=sorted(KERNEL_CHOICES),
+                    help="force the solver's corrective-pass kernel on the timed forms "
+                         "(profiling captures of the other kernels; default: the solver's choice)")
     args = ap.parse_args()
     if args.size:
         _set_size(*(int(v) for v in args.size.split(",")))
+    if args.kernel is not None:
+        _set_kernel(args.kernel)
     if args.acc_steps:
         global ACC_STEPS
         ACC_STEPS = args.acc_steps

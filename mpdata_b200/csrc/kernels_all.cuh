@@ -54,18 +54,6 @@ constexpr int kBX = 32, kBY = 8;
 inline dim3 full_grid(const Dims& d) { return dim3((d.nx + kBX - 1) / kBX, (d.ny + kBY - 1) / kBY, d.ns); }
 }  // namespace
 
-template <typename T>
-void launch_courant(const Dims& d, const T* dx, const T* dy, const T* ds, T dt, const T* u0,
-                    const T* u1, const T* v0, const T* v1, const T* w0, const T* w1, T* U,
-                    T* V, T* W, int k0, int nk, cudaStream_t s)
-{
-    if (nk <= 0) return;
-    dim3 g = full_grid(d);
-    g.z = nk;
-    k_courant<T><<<g, dim3(kBX, kBY), 0, s>>>(d, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, U, V, W,
-                                              k0);
-}
-
 // z-chunk depth of a vector march over `planes` planes with `cols` CTAs per
 // plane and `per_sm` CTAs resident on each of the 148 SMs: the depth that
 // minimises whole waves x (planes per CTA + one plane of setup loads), so
@@ -90,6 +78,25 @@ template <typename K> int resident_per_sm(K kern)
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, 256, 0) != cudaSuccess || n < 1) n = 1;
     return n;
+}
+
+template <typename T>
+void launch_courant(const Dims& d, const T* dx, const T* dy, const T* ds, T dt, const T* u0,
+                    const T* u1, const T* v0, const T* v1, const T* w0, const T* w1, T* U,
+                    T* V, T* W, int k0, int nk, cudaStream_t s)
+{
+    if (nk <= 0) return;
+    // vector march (k_courant_v): 32 x 8 threads of 16 bytes each, z chunks in whole waves
+    constexpr int N = 16 / (int)sizeof(T);
+    const bool one = u0 == u1 && v0 == v1 && w0 == w1;
+    auto kern = one ? k_courant_v<T, true> : k_courant_v<T, false>;
+    static const int per_sm[2] = {resident_per_sm(k_courant_v<T, false>),
+                                  resident_per_sm(k_courant_v<T, true>)};
+    const int gx = (d.nx + 32 * N - 1) / (32 * N), gy = (d.ny + 7) / 8;
+    const int depth = vector_march_depth((long long)gx * gy, nk, per_sm[one]);
+    dim3 g(gx, gy, (nk + depth - 1) / depth);
+    kern<<<g, dim3(32, 8), 0, s>>>(d, dx, dy, ds, dt, u0, u1, v0, v1, w0, w1, U, V, W, depth, k0,
+                                   k0 + nk);
 }
 
 template <typename T>

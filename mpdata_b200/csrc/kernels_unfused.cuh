@@ -339,6 +339,95 @@ template <typename T> __device__ __forceinline__ T mul_rn(T a, T b);
 template <> __device__ __forceinline__ float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
 template <> __device__ __forceinline__ double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
 
+// The advective faces alone (R5: uu.c:126-138, vv.c:137-149, ww.c:143-155)
+// of planes [k0, k1), every entry of those planes written as k_courant
+// writes it (0 where a face does not exist; columns i >= nx untouched), as a
+// z march over 16-byte vectors: QUAT dt / dx[i] and QUAT dt / dy[j] are formed
+// once per thread, QUAT dt / ds[k] once per plane, and the upper z plane of
+// w is carried to the next plane, so each velocity element is read once
+// (ONE_LEVEL: u1, v1, w1 are u0, v0, w0, loaded once).  The operands and
+// their order are k_courant's: the same bits.
+template <typename T, bool ONE_LEVEL>
+__global__ void __launch_bounds__(256) k_courant_v(
+    Dims d, const T* __restrict__ dx, const T* __restrict__ dy, const T* __restrict__ ds, T dt,
+    const T* __restrict__ u0, const T* __restrict__ u1, const T* __restrict__ v0,
+    const T* __restrict__ v1, const T* __restrict__ w0, const T* __restrict__ w1,
+    T* __restrict__ U, T* __restrict__ V, T* __restrict__ W, int depth, int k0, int k1)
+{
+    constexpr int N = Vec16<T>::N;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * N;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i0 >= d.nx || j >= d.ny) return;
+    const int kb = k0 + (int)blockIdx.z * depth, ke = min(k1, kb + depth);
+    const int nx = d.nx, ny = d.ny, ns = d.ns;
+    const long long Y = d.px, Z = d.pp;
+    const T qdt = RealConst<T>::quat * dt;
+    const bool jin = j >= 1 && j <= ny - 2, jv = j <= ny - 2;
+    T rx[N];
+#pragma unroll
+    for (int e = 0; e < N; e++) rx[e] = (i0 + e <= nx - 2) ? ratio<false>(qdt, dx[i0 + e]) : T(0);
+    const T ry = jv ? ratio<false>(qdt, dy[j]) : T(0);
+    // the last lane's x face reads the first velocity of the next vector
+    const bool need_r = i0 + N - 1 <= nx - 2;
+    const bool full = i0 + N <= nx;  // every lane is a cell of the row
+    auto iin = [&](int e) { return i0 + e >= 1 && i0 + e <= nx - 2; };
+    long long q = cell(d, i0, j, kb);
+    Vec16<T> wc0{}, wc1{};  // w of plane k (both time levels), carried
+    if (jin && kb < ke && kb <= ns - 2) {
+        wc0 = ld16(w0 + q);
+        wc1 = ONE_LEVEL ? wc0 : ld16(w1 + q);
+    }
+    for (int k = kb; k < ke; k++, q += Z) {
+        const bool kin = k >= 1 && k <= ns - 2;
+        Vec16<T> uf, vf, wf;
+#pragma unroll
+        for (int e = 0; e < N; e++) uf.v[e] = vf.v[e] = wf.v[e] = T(0);
+        if (kin && jin) {
+            const Vec16<T> a0 = ld16(u0 + q), a1 = ONE_LEVEL ? a0 : ld16(u1 + q);
+            T a0r = T(0), a1r = T(0);
+            if (need_r) {
+                a0r = __ldg(u0 + q + N);
+                a1r = ONE_LEVEL ? a0r : __ldg(u1 + q + N);
+            }
+#pragma unroll
+            for (int e = 0; e < N; e++) {
+                const T r0 = e < N - 1 ? a0.v[e < N - 1 ? e + 1 : 0] : a0r;
+                const T r1 = e < N - 1 ? a1.v[e < N - 1 ? e + 1 : 0] : a1r;
+                if (i0 + e <= nx - 2) uf.v[e] = mul_rn(rx[e], ((a0.v[e] + r0) + a1.v[e]) + r1);
+            }
+        }
+        if (kin && jv) {
+            const Vec16<T> b0 = ld16(v0 + q), b0u = ld16(v0 + q + Y);
+            const Vec16<T> b1 = ONE_LEVEL ? b0 : ld16(v1 + q), b1u = ONE_LEVEL ? b0u : ld16(v1 + q + Y);
+#pragma unroll
+            for (int e = 0; e < N; e++)
+                if (iin(e)) vf.v[e] = mul_rn(ry, ((b0.v[e] + b0u.v[e]) + b1.v[e]) + b1u.v[e]);
+        }
+        if (jin && k <= ns - 2) {
+            const Vec16<T> wp0 = ld16(w0 + q + Z), wp1 = ONE_LEVEL ? wp0 : ld16(w1 + q + Z);
+            const T rz = ratio<false>(qdt, ds[k]);
+#pragma unroll
+            for (int e = 0; e < N; e++)
+                if (iin(e)) wf.v[e] = mul_rn(rz, ((wc0.v[e] + wp0.v[e]) + wc1.v[e]) + wp1.v[e]);
+            wc0 = wp0;
+            wc1 = wp1;
+        }
+        if (full) {
+            st16(U + q, uf);
+            st16(V + q, vf);
+            st16(W + q, wf);
+        } else {
+#pragma unroll
+            for (int e = 0; e < N; e++)
+                if (i0 + e < nx) {
+                    U[q + e] = uf.v[e];
+                    V[q + e] = vf.v[e];
+                    W[q + e] = wf.v[e];
+                }
+        }
+    }
+}
+
 template <typename T, bool ONE_LEVEL>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) k_courant_donor_v(
     Dims d, const T* __restrict__ dx, const T* __restrict__ dy, const T* __restrict__ ds, T dt,

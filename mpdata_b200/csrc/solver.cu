@@ -71,57 +71,100 @@ __device__ __forceinline__ void neu_add(double& s, double& comp, double x)
     s = t;
 }
 
-// Per-block partials over the interior cells: compensated sum, min, count < 0.
-template <typename T>
-__global__ void k_stats(Dims d, const T* __restrict__ c, double* __restrict__ part)
+// Merge the partial (S, C, M, N) in slot b of a 4 x kRedThreads shared
+// array into slot a: Neumaier sum of the sums, compensations added, min,
+// count.
+__device__ __forceinline__ void stats_merge(double (*sh)[kRedThreads], int a, int b)
 {
-    const long long nint = (long long)(d.nx - 2) * (d.ny - 2) * (d.ns - 2);
-    double s = 0, comp = 0, mn = 1e308, neg = 0;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint;
-         t += (long long)gridDim.x * blockDim.x) {
-        int i = 1 + (int)(t % (d.nx - 2));
-        long long r = t / (d.nx - 2);
-        int j = 1 + (int)(r % (d.ny - 2));
-        int k = 1 + (int)(r / (d.ny - 2));
-        double x = (double)c[cell(d, i, j, k)];
-        neu_add(s, comp, x);
-        mn = x < mn ? x : mn;
-        neg += x < 0 ? 1.0 : 0.0;
-    }
-    __shared__ double sh[4][kRedThreads];
-    sh[0][threadIdx.x] = s;
-    sh[1][threadIdx.x] = comp;
-    sh[2][threadIdx.x] = mn;
-    sh[3][threadIdx.x] = neg;
+    neu_add(sh[0][a], sh[1][a], sh[0][b]);
+    sh[1][a] += sh[1][b];
+    sh[2][a] = sh[2][b] < sh[2][a] ? sh[2][b] : sh[2][a];
+    sh[3][a] += sh[3][b];
+}
+
+// Fixed-order tree over the block's kRedThreads slots (deterministic); slot 0
+// holds the result.
+__device__ __forceinline__ void stats_tree(double (*sh)[kRedThreads])
+{
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double S = 0, Cp = 0, M = 1e308, N = 0;
-        for (int q = 0; q < kRedThreads; q++) {  // fixed order: deterministic
-            neu_add(S, Cp, sh[0][q]);
-            Cp += sh[1][q];
-            M = sh[2][q] < M ? sh[2][q] : M;
-            N += sh[3][q];
-        }
-        part[4 * blockIdx.x + 0] = S;
-        part[4 * blockIdx.x + 1] = Cp;
-        part[4 * blockIdx.x + 2] = M;
-        part[4 * blockIdx.x + 3] = N;
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) stats_merge(sh, threadIdx.x, threadIdx.x + w);
+        __syncthreads();
     }
 }
 
-__global__ void k_stats_final(const double* __restrict__ part, int nblk, double* __restrict__ out)
+// Per-block partials over the interior cells: compensated sum, min, count < 0.
+// One warp per interior row (rows spread over the blocks in a fixed order),
+// lanes along x with four loads in flight; no per-element index arithmetic.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_stats(Dims d, const T* __restrict__ c,
+                                                       double* __restrict__ part)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    constexpr int NW = kRedThreads / 32;
+    const int nxi = d.nx - 2, nyi = d.ny - 2;
+    const long long rows = (long long)nyi * (d.ns - 2);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // four independent compensated sums per thread (the loads of one group
+    // of four feed four dependency chains), merged in a fixed order
+    double s[4] = {0, 0, 0, 0}, comp[4] = {0, 0, 0, 0}, mn = 1e308;
+    long long neg = 0;
+    auto acc = [&](int a, double x) {
+        neu_add(s[a], comp[a], x);
+        mn = x < mn ? x : mn;
+        neg += x < 0 ? 1 : 0;
+    };
+    for (long long r = (long long)blockIdx.x * NW + warp; r < rows; r += (long long)gridDim.x * NW) {
+        const int j = 1 + (int)(r % nyi), k = 1 + (int)(r / nyi);
+        const T* row = c + cell(d, 1, j, k);
+        int i = lane;
+        for (; i + 96 < nxi; i += 128) {
+            const double x0 = (double)row[i], x1 = (double)row[i + 32], x2 = (double)row[i + 64],
+                         x3 = (double)row[i + 96];
+            acc(0, x0);
+            acc(1, x1);
+            acc(2, x2);
+            acc(3, x3);
+        }
+        for (; i < nxi; i += 32) acc(0, (double)row[i]);
+    }
+#pragma unroll
+    for (int a = 1; a < 4; a++) {
+        neu_add(s[0], comp[0], s[a]);
+        comp[0] += comp[a];
+    }
+    __shared__ double sh[4][kRedThreads];
+    sh[0][threadIdx.x] = s[0];
+    sh[1][threadIdx.x] = comp[0];
+    sh[2][threadIdx.x] = mn;
+    sh[3][threadIdx.x] = (double)neg;
+    stats_tree(sh);
+    if (threadIdx.x < 4) part[4 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// One block of kRedThreads: thread t merges the partials t, t + kRedThreads,
+// ... in order, then the fixed-order tree (deterministic).
+__global__ void __launch_bounds__(kRedThreads) k_stats_final(const double* __restrict__ part,
+                                                             int nblk, double* __restrict__ out)
+{
+    __shared__ double sh[4][kRedThreads];
+    const int t = threadIdx.x;
     double S = 0, Cp = 0, M = 1e308, N = 0;
-    for (int b = 0; b < nblk; b++) {
+    for (int b = t; b < nblk; b += kRedThreads) {
         neu_add(S, Cp, part[4 * b + 0]);
         Cp += part[4 * b + 1];
         M = part[4 * b + 2] < M ? part[4 * b + 2] : M;
         N += part[4 * b + 3];
     }
-    out[0] = S + Cp;
-    out[1] = M;
-    out[2] = N;
+    sh[0][t] = S;
+    sh[1][t] = Cp;
+    sh[2][t] = M;
+    sh[3][t] = N;
+    stats_tree(sh);
+    if (t == 0) {
+        out[0] = sh[0][0] + sh[1][0];
+        out[1] = sh[2][0];
+        out[2] = sh[3][0];
+    }
 }
 
 // max |face| over the three face arrays, whole (unused entries hold 0).
@@ -146,12 +189,19 @@ __global__ void k_facemax(Dims d, const T* __restrict__ U, const T* __restrict__
     if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
-__global__ void k_max_final(const double* __restrict__ part, int nblk, double* __restrict__ out)
+__global__ void __launch_bounds__(kRedThreads) k_max_final(const double* __restrict__ part,
+                                                           int nblk, double* __restrict__ out)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    __shared__ double sh[kRedThreads];
     double m = 0;
-    for (int b = 0; b < nblk; b++) m = fmax(m, part[b]);
-    out[0] = m;
+    for (int b = threadIdx.x; b < nblk; b += kRedThreads) m = fmax(m, part[b]);
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sh[0];
 }
 
 }  // namespace
@@ -266,7 +316,8 @@ template <typename T> int check_courant(Solver* h)
 {
     mpd::k_facemax<T><<<mpd::kRedBlocks, mpd::kRedThreads, 0, h->stream>>>(
         h->d, F<T>(h, 0, 0), F<T>(h, 0, 1), F<T>(h, 0, 2), h->red);
-    mpd::k_max_final<<<1, 1, 0, h->stream>>>(h->red, mpd::kRedBlocks, h->red + 4 * mpd::kRedBlocks);
+    mpd::k_max_final<<<1, mpd::kRedThreads, 0, h->stream>>>(h->red, mpd::kRedBlocks,
+                                                            h->red + 4 * mpd::kRedBlocks);
     double m = 0;
     CUDA_TRY(cudaMemcpyAsync(&m, h->red + 4 * mpd::kRedBlocks, sizeof m, cudaMemcpyDeviceToHost,
                              h->stream));
@@ -879,7 +930,8 @@ int mpd::stats(Solver* h, double out[3])
     else
         mpd::k_stats<double><<<mpd::kRedBlocks, mpd::kRedThreads, 0, h->stream>>>(
             h->d, (const double*)h->c[h->cur], h->red);
-    mpd::k_stats_final<<<1, 1, 0, h->stream>>>(h->red, mpd::kRedBlocks, h->red + 4 * mpd::kRedBlocks);
+    mpd::k_stats_final<<<1, mpd::kRedThreads, 0, h->stream>>>(h->red, mpd::kRedBlocks,
+                                                              h->red + 4 * mpd::kRedBlocks);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, h->red + 4 * mpd::kRedBlocks, 3 * sizeof(double),
                              cudaMemcpyDeviceToHost, h->stream));

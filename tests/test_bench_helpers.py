@@ -53,3 +53,19 @@ def test_reference_arm_loads_workloads_without_the_library():
         "assert 'mpdata_b200' not in sys.modules\n" % ROOT)
     p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
     assert p.returncode == 0, p.stderr
+
+
+def test_kernel_option_keeps_the_forms_the_kernel_runs():
+    """--kernel 1 (one kernel per reference routine) keeps only the IEEE form
+    (approx_div needs the fused kernels) and labels the roofline kernel."""
+    code = ("import bench; bench._set_kernel(1); "
+            "print([n for n, _ in bench.FORMS], bench.FORMS[0][1]['kernel'], "
+            "bench.KERNEL_OF_FORM['plain'].split()[0])")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                         check=True).stdout.split()
+    assert out == ["['plain']", "1", "k_antidiff"]
+    code = ("import bench; bench._set_kernel(2); print(len(bench.FORMS), "
+            "all(o['kernel'] == 2 for _, o in bench.FORMS))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                         check=True).stdout.split()
+    assert out == ["3", "True"]
