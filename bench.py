@@ -108,6 +108,12 @@ def _set_kernel(kernel):
         KERNEL_OF_FORM = {n: KERNEL_CHOICES[kernel] for n, _ in FORMS}
 
 
+def _add_form_options(**kw):
+    """Options added to every timed form (profiling captures)."""
+    global FORMS
+    FORMS = [(n, dict(o, **kw)) for n, o in FORMS]
+
+
 def config_text():
     return (f"roofline: {NX}x{NY}x{NS} FP32, IORD {ORDER} + nonoscillatory limiter, "
             "streamfunction flow, y faces of the x = 1 column computed (vv_fix)")
@@ -1015,7 +1021,12 @@ def main():
     ap.add_argument("--kernel", type=int, default=None, choices=sorted(KERNEL_CHOICES),
                     help="force the solver's corrective-pass kernel on the timed forms "
                          "(profiling captures of the other kernels; default: the solver's choice)")
+    ap.add_argument("--check-courant", action="store_true",
+                    help="the timed forms run with the Courant check (profiling captures of "
+                         "its kernels)")
     args = ap.parse_args()
+    if args.check_courant:
+        _add_form_options(check_courant=True)
     if args.size:
         _set_size(*(int(v) for v in args.size.split(",")))
     if args.kernel is not None:

@@ -167,23 +167,39 @@ __global__ void __launch_bounds__(kRedThreads) k_stats_final(const double* __res
     }
 }
 
-// max |face| over the three face arrays, whole (unused entries hold 0).
+// max |face| over the three face arrays, whole (unused entries hold 0):
+// 16-byte loads (every array is a multiple of 32 elements, 256-byte
+// aligned), three independent maxima per thread.
+template <typename T> struct Vec16Of;
+template <> struct Vec16Of<float> { using type = float4; };
+template <> struct Vec16Of<double> { using type = double2; };
+__device__ __forceinline__ double vabsmax(float4 v)
+{
+    return fmax(fmax(fabs((double)v.x), fabs((double)v.y)), fmax(fabs((double)v.z), fabs((double)v.w)));
+}
+__device__ __forceinline__ double vabsmax(double2 v) { return fmax(fabs(v.x), fabs(v.y)); }
+
 template <typename T>
 __global__ void k_facemax(Dims d, const T* __restrict__ U, const T* __restrict__ V,
                           const T* __restrict__ W, double* __restrict__ part)
 {
-    const long long n = (long long)d.pp * d.ns;
-    double m = 0;
+    using VT = typename Vec16Of<T>::type;
+    const long long n = (long long)d.pp * d.ns / (long long)(16 / sizeof(T));
+    const VT* u = reinterpret_cast<const VT*>(U);
+    const VT* v = reinterpret_cast<const VT*>(V);
+    const VT* w = reinterpret_cast<const VT*>(W);
+    double ma = 0, mb = 0, mc = 0;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
-        double a = fabs((double)U[t]), b = fabs((double)V[t]), c = fabs((double)W[t]);
-        m = fmax(m, fmax(a, fmax(b, c)));
+        ma = fmax(ma, vabsmax(u[t]));
+        mb = fmax(mb, vabsmax(v[t]));
+        mc = fmax(mc, vabsmax(w[t]));
     }
     __shared__ double sh[kRedThreads];
-    sh[threadIdx.x] = m;
+    sh[threadIdx.x] = fmax(ma, fmax(mb, mc));
     __syncthreads();
-    for (int w = kRedThreads / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + w]);
+    for (int k = kRedThreads / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + k]);
         __syncthreads();
     }
     if (threadIdx.x == 0) part[blockIdx.x] = sh[0];

@@ -69,3 +69,11 @@ def test_kernel_option_keeps_the_forms_the_kernel_runs():
     out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
                          check=True).stdout.split()
     assert out == ["3", "True"]
+
+
+def test_check_courant_option_reaches_every_form():
+    code = ("import bench; bench._add_form_options(check_courant=True); "
+            "print(all(o.get('check_courant') for _, o in bench.FORMS), len(bench.FORMS))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                         check=True).stdout.split()
+    assert out == ["True", "3"]
